@@ -1,0 +1,113 @@
+/*
+ * CPU restatement of the reference's walk hot path and SGNS updates.
+ *
+ * TEST INFRASTRUCTURE ONLY: the checker that the CUDA library is compared
+ * against.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
+ * load it; the shipped library never links or calls it.
+ *
+ * Walk parity is pinned against the reference itself: with the stream random
+ * source (dgo_stream_*), dgo_walk_rounds() reproduces, byte for byte, the walk
+ * files of the unmodified reference engine built by `make -C oracle ref`
+ * (oracle/_ref/ref_walk, one worker thread, pinned mt19937 seed).
+ */
+#ifndef DG_ORACLE_H
+#define DG_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Directed CSR built exactly as include/graph.hpp:642-824 + 509-540 build it
+ * for one partition: optional undirected doubling in record order
+ * (graph.hpp:671-686), out/in degrees (694-717), neighbours bucketed by source in
+ * edge order (build_edge_container, 509-540). */
+typedef struct {
+    uint32_t v_num;
+    uint64_t m;
+    uint64_t *offsets;  /* v_num + 1 */
+    uint32_t *nbr;      /* m */
+    float *data;        /* m */
+    uint32_t *out_deg;  /* v_num */
+    uint32_t *in_deg;   /* v_num */
+} dgo_csr;
+
+typedef struct {
+    uint32_t src, dst;
+    float data;
+} dgo_edge;
+
+int dgo_csr_build(const dgo_edge *edges, uint64_t n_edges, uint32_t v_num, int undirected, dgo_csr *out);
+void dgo_csr_free(dgo_csr *g);
+
+/* Random source for the walk. */
+enum { DGO_RNG_PHILOX = 0, DGO_RNG_CALLBACK = 1 };
+typedef uint32_t (*dgo_cand_fn)(void *ctx, uint32_t degree);
+typedef uint32_t (*dgo_acc_fn)(void *ctx);
+
+typedef struct {
+    uint32_t min_len;    /* --min_L, walk.hpp:404 */
+    uint32_t init_round; /* --min_R, walk.hpp:405 */
+    uint32_t walker_num; /* -w */
+    uint32_t rounds;     /* last round index; the reference stops after 30 (walk.hpp:740) */
+    uint64_t seed;       /* Philox key */
+    int rng_mode;
+    dgo_cand_fn cand_cb; /* DGO_RNG_CALLBACK only */
+    dgo_acc_fn acc_cb;
+    void *cb_ctx;
+} dgo_walk_params;
+
+typedef struct {
+    uint64_t footprints;  /* all footprints, start vertices included */
+    uint64_t steps;       /* footprints with step >= 1: the reference's p_step (walk.hpp:864,962,988) */
+    uint64_t draws;       /* candidate draws (transition attempts) */
+    uint64_t traces;      /* rejected candidates: walk.hpp:938-942 trace_num */
+    uint64_t pow_sq_mismatch; /* R values where pow(R,2) != R*R (expected 0) */
+    uint64_t near_ties;   /* draws with |tanh(p_accept) - p| < 1e-12 */
+    uint32_t max_len;     /* longest walk, in footprints */
+} dgo_walk_stats;
+
+/* Walks of one round: walker w starts at w % v_num (walk.hpp:501-509). */
+typedef struct {
+    uint32_t n_walks;
+    uint64_t total;
+    uint64_t *offsets; /* n_walks + 1 */
+    uint32_t *verts;   /* total */
+} dgo_paths;
+
+/* Advances walkers [0, n_walkers) of `round` to completion, in ascending id order
+ * (the order a one-worker reference run uses), following walk.hpp:845-1024. */
+int dgo_walk_round(const dgo_csr *g, const dgo_walk_params *p, uint32_t round, uint32_t n_walkers,
+                   dgo_paths *out, dgo_walk_stats *stats);
+void dgo_paths_free(dgo_paths *p);
+
+/* Writes one walk per line as " %u" per vertex then "\n" (path.hpp:67-119). */
+int dgo_write_walks(const char *path, const dgo_paths *p);
+
+/* Relative entropy of cumulative visit frequency vs out-degree share
+ * (walk.hpp:694-725), natural log, summed in vertex order. */
+double dgo_relative_entropy(const uint32_t *out_deg, const uint32_t *freq, uint32_t v_num);
+
+/* Per-CSR-entry acceptance threshold: the smallest k in [0, 2^31-1] with
+ * tanh(p_accept) <= k / 2147483647.0 (glibc tanh), or 2^31 when none exists. */
+void dgo_thresholds(const dgo_csr *g, uint32_t *thr);
+
+/* t(Sn, fi) = log2(A(Sn) * B(fi)) as Correlation::iterateHn computes it
+ * (walk.hpp:284-303), tabulated for 1 <= Sn <= max_sn, 0 <= fi <= Sn at index
+ * Sn*(Sn+1)/2 + fi - 1. */
+void dgo_entropy_table(uint32_t max_sn, double *out);
+uint64_t dgo_entropy_table_size(uint32_t max_sn);
+
+/* The reference's candidate / acceptance streams for the pin test:
+ * std::mt19937(seed) + std::uniform_int_distribution<uint32_t>(0, degree-1)
+ * (util.hpp:37-41) and glibc rand() from its default state (walk.hpp:928). */
+void *dgo_stream_new(uint32_t seed);
+void dgo_stream_free(void *s);
+uint32_t dgo_stream_cand(void *s, uint32_t degree);
+uint32_t dgo_stream_acc(void *s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

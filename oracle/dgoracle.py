@@ -1,0 +1,179 @@
+"""ctypes front end of the CPU checker (oracle/libdgoracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the shipped library.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libdgoracle.so")
+REF_WALK = os.path.join(HERE, "_ref", "ref_walk")
+REF_WALK_FMA = os.path.join(HERE, "_ref", "ref_walk_fma")
+
+EDGE_DTYPE = np.dtype([("src", "<u4"), ("dst", "<u4"), ("data", "<f4")])
+
+
+class _Csr(C.Structure):
+    _fields_ = [("v_num", C.c_uint32), ("m", C.c_uint64), ("offsets", C.POINTER(C.c_uint64)),
+                ("nbr", C.POINTER(C.c_uint32)), ("data", C.POINTER(C.c_float)),
+                ("out_deg", C.POINTER(C.c_uint32)), ("in_deg", C.POINTER(C.c_uint32))]
+
+
+class _WalkParams(C.Structure):
+    _fields_ = [("min_len", C.c_uint32), ("init_round", C.c_uint32), ("walker_num", C.c_uint32),
+                ("rounds", C.c_uint32), ("seed", C.c_uint64), ("rng_mode", C.c_int),
+                ("cand_cb", C.c_void_p), ("acc_cb", C.c_void_p), ("cb_ctx", C.c_void_p)]
+
+
+class WalkStats(C.Structure):
+    _fields_ = [("footprints", C.c_uint64), ("steps", C.c_uint64), ("draws", C.c_uint64),
+                ("traces", C.c_uint64), ("pow_sq_mismatch", C.c_uint64), ("near_ties", C.c_uint64),
+                ("max_len", C.c_uint32)]
+
+
+class _Paths(C.Structure):
+    _fields_ = [("n_walks", C.c_uint32), ("total", C.c_uint64), ("offsets", C.POINTER(C.c_uint64)),
+                ("verts", C.POINTER(C.c_uint32))]
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def build_ref() -> bool:
+    """Compile the reference's walk engine into oracle/_ref (needs the reference tree)."""
+    if os.path.exists(REF_WALK) and os.path.exists(REF_WALK_FMA):
+        return True
+    ref = os.environ.get("DG_REFERENCE_DIR", "/root/reference")
+    if not os.path.isdir(os.path.join(ref, "include")):
+        return False
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
+    return True
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.dgo_csr_build.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.POINTER(_Csr)]
+        L.dgo_csr_free.argtypes = [C.POINTER(_Csr)]
+        L.dgo_walk_round.argtypes = [C.POINTER(_Csr), C.POINTER(_WalkParams), C.c_uint32, C.c_uint32,
+                                     C.POINTER(_Paths), C.POINTER(WalkStats)]
+        L.dgo_paths_free.argtypes = [C.POINTER(_Paths)]
+        L.dgo_write_walks.argtypes = [C.c_char_p, C.POINTER(_Paths)]
+        L.dgo_relative_entropy.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        L.dgo_relative_entropy.restype = C.c_double
+        L.dgo_thresholds.argtypes = [C.POINTER(_Csr), C.c_void_p]
+        L.dgo_entropy_table.argtypes = [C.c_uint32, C.c_void_p]
+        L.dgo_entropy_table_size.argtypes = [C.c_uint32]
+        L.dgo_entropy_table_size.restype = C.c_uint64
+        L.dgo_stream_new.argtypes = [C.c_uint32]
+        L.dgo_stream_new.restype = C.c_void_p
+        L.dgo_stream_free.argtypes = [C.c_void_p]
+        _lib = L
+    return _lib
+
+
+def _u32(ptr, n):
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy() if n else np.zeros(0, np.uint32)
+
+
+class Csr:
+    """Directed CSR exactly as the reference builds it for one partition."""
+
+    def __init__(self, edges: np.ndarray, v_num: int, undirected: bool = True):
+        edges = np.ascontiguousarray(edges, dtype=EDGE_DTYPE)
+        self._c = _Csr()
+        rc = lib().dgo_csr_build(edges.ctypes.data, edges.size, v_num, int(undirected), C.byref(self._c))
+        if rc:
+            raise ValueError(f"dgo_csr_build failed ({rc})")
+        m = self._c.m
+        self.v_num = v_num
+        self.m = m
+        self.offsets = np.ctypeslib.as_array(self._c.offsets, shape=(v_num + 1,)).copy()
+        self.nbr = _u32(self._c.nbr, m)
+        self.data = np.ctypeslib.as_array(self._c.data, shape=(m,)).copy() if m else np.zeros(0, np.float32)
+        self.out_deg = _u32(self._c.out_deg, v_num)
+        self.in_deg = _u32(self._c.in_deg, v_num)
+
+    def thresholds(self) -> np.ndarray:
+        out = np.empty(self.m, dtype=np.uint32)
+        lib().dgo_thresholds(C.byref(self._c), out.ctypes.data)
+        return out
+
+    def __del__(self):
+        try:
+            lib().dgo_csr_free(C.byref(self._c))
+        except Exception:
+            pass
+
+
+def walk_rounds(csr: Csr, walker_num: int, min_len: int = 20, init_round: int = 5, rounds: int = 30,
+                seed: int = 0, stream_seed: int | None = None, first_round: int = 1,
+                round_walkers=None):
+    """Run rounds first_round..rounds as internal_random_walk does (walk.hpp:609-782).
+
+    Returns (list of (offsets, verts) per round, WalkStats).  With stream_seed set,
+    the reference's mt19937/rand() streams are consumed in one-worker order
+    instead of Philox.
+    """
+    L = lib()
+    p = _WalkParams(min_len=min_len, init_round=init_round, walker_num=walker_num, rounds=rounds,
+                    seed=seed, rng_mode=0)
+    ctx = None
+    if stream_seed is not None:
+        ctx = L.dgo_stream_new(stream_seed)
+        p.rng_mode = 1
+        p.cand_cb = C.cast(L.dgo_stream_cand, C.c_void_p).value
+        p.acc_cb = C.cast(L.dgo_stream_acc, C.c_void_p).value
+        p.cb_ctx = ctx
+    stats = WalkStats()
+    out = []
+    try:
+        for r in range(first_round, rounds + 1):
+            n = round_walkers(r) if round_walkers else (walker_num * init_round if r == 1 else walker_num)
+            paths = _Paths()
+            rc = L.dgo_walk_round(C.byref(csr._c), C.byref(p), r, n, C.byref(paths), C.byref(stats))
+            if rc:
+                raise RuntimeError(f"dgo_walk_round failed ({rc})")
+            offs = np.ctypeslib.as_array(paths.offsets, shape=(n + 1,)).copy()
+            verts = _u32(paths.verts, paths.total)
+            L.dgo_paths_free(C.byref(paths))
+            out.append((offs, verts))
+    finally:
+        if ctx is not None:
+            L.dgo_stream_free(ctx)
+    return out, stats
+
+
+def walk_text(offsets: np.ndarray, verts: np.ndarray) -> bytes:
+    """Walk file bytes: " %u" per vertex, "\\n" per walk (path.hpp:92,108)."""
+    parts = []
+    for w in range(offsets.size - 1):
+        seg = verts[offsets[w]:offsets[w + 1]]
+        parts.append("".join(" %d" % x for x in seg.tolist()) + "\n")
+    return "".join(parts).encode()
+
+
+def relative_entropy(out_deg: np.ndarray, freq: np.ndarray) -> float:
+    out_deg = np.ascontiguousarray(out_deg, dtype=np.uint32)
+    freq = np.ascontiguousarray(freq, dtype=np.uint32)
+    return lib().dgo_relative_entropy(out_deg.ctypes.data, freq.ctypes.data, out_deg.size)
+
+
+def entropy_table(max_sn: int) -> np.ndarray:
+    n = lib().dgo_entropy_table_size(max_sn)
+    out = np.empty(n, dtype=np.float64)
+    lib().dgo_entropy_table(max_sn, out.ctypes.data)
+    return out

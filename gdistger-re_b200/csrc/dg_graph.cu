@@ -1,0 +1,268 @@
+// Graph loading: binary edge records -> device CSR with per-entry acceptance
+// thresholds, plus the entropy-term table the walk kernel reads.
+#include "dg_internal.h"
+
+#include <cerrno>
+#include <climits>
+#include <cmath>
+#include <cstring>
+#include <memory>
+
+namespace {
+
+constexpr uint32_t kRandMax = 2147483647u;  // glibc RAND_MAX, walk.hpp:928
+constexpr uint32_t kNever = 0x80000000u;    // threshold no 31-bit draw reaches
+
+struct HostEdge {
+    uint32_t src, dst;
+    float data;
+};
+static_assert(sizeof(HostEdge) == 12, "edge records are 12 bytes (storage.hpp:15-37)");
+
+// Smallest k in [0, 2^31 - 1] with t <= k / 2147483647.0, the draw at which the
+// reference's `p_norm <= p` (walk.hpp:938) first holds.  The guess is within one
+// or two of the answer; the corrections are capped for safety.
+__device__ uint32_t threshold_of(double t) {
+    if (isnan(t)) return kNever;
+    if (t <= 0.0) return 0u;
+    if (t > 1.0) return kNever;
+    long long k = (long long)ceil(__dmul_rn(t, (double)kRandMax));
+    if (k > (long long)kRandMax) k = kRandMax;
+    if (k < 0) k = 0;
+    for (int i = 0; i < 64 && k > 0 && t <= __ddiv_rn((double)(k - 1), (double)kRandMax); i++) k--;
+    for (int i = 0; i < 64 && k <= (long long)kRandMax && !(t <= __ddiv_rn((double)k, (double)kRandMax)); i++) k++;
+    return k > (long long)kRandMax ? kNever : (uint32_t)k;
+}
+
+// One warp per source vertex: p_accept = (1 / (sd - cn)) * max(sd, dd) / min(sd, dd),
+// p_norm = tanh(p_accept) (walk.hpp:920-934), folded into an integer threshold so
+// that the walk's accept test is a single compare against its 31-bit draw.
+__global__ void threshold_kernel(const uint64_t *__restrict__ offsets, const uint32_t *__restrict__ nbr,
+                                 const float *__restrict__ data, const uint32_t *__restrict__ deg,
+                                 uint32_t v_num, uint2 *__restrict__ entries) {
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warp = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t n_warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < v_num; v += n_warps) {
+        const int sd = (int)deg[v];
+        const uint64_t end = offsets[v + 1];
+        for (uint64_t e = offsets[v] + lane; e < end; e += 32) {
+            const uint32_t dst = nbr[e];
+            const int cn = __float2int_rz(data[e]);
+            const int dd = (int)deg[dst];
+            const int hi = sd > dd ? sd : dd, lo = sd < dd ? sd : dd;
+            const double p_accept =
+                __ddiv_rn(__dmul_rn(__ddiv_rn(1.0, (double)(sd - cn)), (double)hi), (double)lo);
+            entries[e] = make_uint2(dst, threshold_of(tanh(p_accept)));
+        }
+    }
+}
+
+// Correlation::SnSn_div_Snp1Snp1 / FjFj_div_FiFi / iterateHn (walk.hpp:284-304):
+// the log2 term depends only on the integers (Sn, fi), so the host tabulates it
+// once with the C library's pow/log2 -- the same functions the reference calls.
+double entropy_term(double Sn, double fi) {
+    const double k = 1.0;
+    double Snp1 = Sn + k;
+    double a = std::pow(Sn / Snp1, Sn) * std::pow(1.0 / Snp1, k);
+    if (fi == 0) return std::log2(a);
+    double fj = fi + k;
+    double b = std::pow(fj / fi, fi) * std::pow(fj, k);
+    return std::log2(a * b);
+}
+
+int build_graph(const HostEdge *edges, uint64_t n_edges, uint32_t v_num, int undirected, int device,
+                dg_graph **out) {
+    DG_CHECK(out != nullptr, DG_ERR_ARG, "dg_graph_create: out is NULL");
+    *out = nullptr;
+    DG_CHECK(v_num > 0, DG_ERR_ARG, "dg_graph_create: v_num must be positive");
+    int n_dev = 0;
+    DG_CUDA(cudaGetDeviceCount(&n_dev));
+    DG_CHECK(device >= 0 && device < n_dev, DG_ERR_ARG, "dg_graph_create: device %d out of range (%d)", device, n_dev);
+    // Validate records the way the reference's asserts would fail (graph.hpp:639,
+    // walk.hpp:920 converts data to int).
+    for (uint64_t i = 0; i < n_edges; i++) {
+        const HostEdge &e = edges[i];
+        DG_CHECK(e.src < v_num && e.dst < v_num, DG_ERR_ARG,
+                 "edge %llu (%u, %u) has a vertex id >= v_num = %u", (unsigned long long)i, e.src, e.dst, v_num);
+        DG_CHECK(std::isfinite(e.data) && e.data > -2147483648.0f && e.data < 2147483648.0f, DG_ERR_ARG,
+                 "edge %llu has data %g outside the int range the transition converts it to",
+                 (unsigned long long)i, (double)e.data);
+    }
+    const uint64_t m = undirected ? 2 * n_edges : n_edges;
+    DG_CHECK(m < (1ull << 40), DG_ERR_ARG, "too many edges");
+
+    // CSR in record order (graph.hpp:671-686 doubling, 509-540 bucketing).
+    std::vector<uint32_t> out_deg(v_num, 0), in_deg(v_num, 0);
+    for (uint64_t i = 0; i < n_edges; i++) {
+        out_deg[edges[i].src]++;
+        in_deg[edges[i].dst]++;
+        if (undirected) {
+            out_deg[edges[i].dst]++;
+            in_deg[edges[i].src]++;
+        }
+    }
+    std::vector<uint64_t> offsets((size_t)v_num + 1, 0);
+    for (uint32_t v = 0; v < v_num; v++) offsets[v + 1] = offsets[v] + out_deg[v];
+    std::vector<uint32_t> nbr(m ? m : 1);
+    std::vector<float> data(m ? m : 1);
+    {
+        std::vector<uint64_t> cursor(offsets.begin(), offsets.end() - 1);
+        for (uint64_t i = 0; i < n_edges; i++) {
+            const HostEdge &e = edges[i];
+            uint64_t at = cursor[e.src]++;
+            nbr[at] = e.dst;
+            data[at] = e.data;
+            if (undirected) {
+                at = cursor[e.dst]++;
+                nbr[at] = e.src;
+                data[at] = e.data;
+            }
+        }
+    }
+
+    dg::DeviceGuard guard(device);
+    std::unique_ptr<dg_graph> g(new dg_graph());
+    g->device = device;
+    g->v_num = v_num;
+    g->m = m;
+    DG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    DG_CUDA(g->offsets.alloc((size_t)v_num + 1));
+    DG_CUDA(g->entries.alloc(m));
+    DG_CUDA(g->out_deg.alloc(v_num));
+    DG_CUDA(g->in_deg.alloc(v_num));
+    DG_CUDA(g->freq.alloc(v_num));
+    DG_CUDA(cudaMemcpyAsync(g->offsets.p, offsets.data(), offsets.size() * 8, cudaMemcpyHostToDevice, g->stream));
+    DG_CUDA(cudaMemcpyAsync(g->out_deg.p, out_deg.data(), (size_t)v_num * 4, cudaMemcpyHostToDevice, g->stream));
+    DG_CUDA(cudaMemcpyAsync(g->in_deg.p, in_deg.data(), (size_t)v_num * 4, cudaMemcpyHostToDevice, g->stream));
+    DG_CUDA(cudaMemsetAsync(g->freq.p, 0, (size_t)v_num * 4, g->stream));
+    if (m) {
+        dg::DevArray<uint32_t> d_nbr;
+        dg::DevArray<float> d_data;
+        DG_CUDA(d_nbr.alloc(m));
+        DG_CUDA(d_data.alloc(m));
+        DG_CUDA(cudaMemcpyAsync(d_nbr.p, nbr.data(), m * 4, cudaMemcpyHostToDevice, g->stream));
+        DG_CUDA(cudaMemcpyAsync(d_data.p, data.data(), m * 4, cudaMemcpyHostToDevice, g->stream));
+        dg::EventTimer t;
+        t.start(g->stream);
+        int blocks = dg::sm_count(device) * 8;
+        threshold_kernel<<<blocks, 256, 0, g->stream>>>(g->offsets.p, d_nbr.p, d_data.p, g->out_deg.p, v_num,
+                                                        g->entries.p);
+        DG_CUDA(cudaGetLastError());
+        t.stop(g->stream);
+        DG_CUDA(cudaStreamSynchronize(g->stream));
+        g->threshold_ms = t.ms();
+    }
+    DG_CUDA(cudaStreamSynchronize(g->stream));
+    g->h_out_deg.swap(out_deg);
+    *out = g.release();
+    return DG_OK;
+}
+
+}  // namespace
+
+dg_graph::~dg_graph() {
+    if (stream) {
+        dg::DeviceGuard guard(device);
+        cudaStreamSynchronize(stream);
+        offsets.release();
+        entries.release();
+        out_deg.release();
+        in_deg.release();
+        freq.release();
+        etable.release();
+        cudaStreamDestroy(stream);
+    }
+}
+
+namespace dg {
+
+int ensure_entropy_table(dg_graph *g, uint32_t max_sn) {
+    if (g->etable_max_sn >= max_sn && g->etable.p) return DG_OK;
+    const uint64_t n = (uint64_t)max_sn * (max_sn + 1) / 2 + max_sn;
+    std::vector<double> t(n);
+    for (uint32_t s = 1; s <= max_sn; s++)
+        for (uint32_t f = 0; f <= s; f++) t[(uint64_t)s * (s + 1) / 2 + f - 1] = entropy_term((double)s, (double)f);
+    DG_CUDA(g->etable.alloc(n));
+    DG_CUDA(cudaMemcpyAsync(g->etable.p, t.data(), n * 8, cudaMemcpyHostToDevice, g->stream));
+    DG_CUDA(cudaStreamSynchronize(g->stream));
+    g->etable_max_sn = max_sn;
+    return DG_OK;
+}
+
+}  // namespace dg
+
+extern "C" int dg_graph_create_from_edges(const void *edges, uint64_t n_edges, uint32_t v_num, int undirected,
+                                          int device, dg_graph **out) {
+    DG_CHECK(edges != nullptr || n_edges == 0, DG_ERR_ARG, "dg_graph_create_from_edges: edges is NULL");
+    return build_graph(static_cast<const HostEdge *>(edges), n_edges, v_num, undirected, device, out);
+}
+
+extern "C" int dg_graph_create(const char *edge_path, uint32_t v_num, int undirected, int device, dg_graph **out) {
+    DG_CHECK(edge_path != nullptr, DG_ERR_ARG, "dg_graph_create: path is NULL");
+    FILE *f = fopen(edge_path, "rb");
+    DG_CHECK(f != nullptr, DG_ERR_IO, "cannot open %s: %s", edge_path, strerror(errno));
+    fseek(f, 0, SEEK_END);
+    long long size = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    if (size < 0 || size % (long long)sizeof(HostEdge) != 0) {
+        fclose(f);
+        return dg::fail(DG_ERR_IO, "%s: size %lld is not a multiple of 12-byte edge records", edge_path, size);
+    }
+    uint64_t n = (uint64_t)size / sizeof(HostEdge);
+    std::vector<HostEdge> edges(n ? n : 1);
+    size_t got = n ? fread(edges.data(), sizeof(HostEdge), n, f) : 0;
+    fclose(f);
+    DG_CHECK(got == n, DG_ERR_IO, "%s: short read (%zu of %llu records)", edge_path, got, (unsigned long long)n);
+    return build_graph(edges.data(), n, v_num, undirected, device, out);
+}
+
+extern "C" void dg_graph_free(dg_graph *g) { delete g; }
+
+extern "C" int dg_graph_get_info(const dg_graph *g, dg_graph_info *info) {
+    DG_CHECK(g && info, DG_ERR_ARG, "dg_graph_get_info: NULL argument");
+    info->v_num = g->v_num;
+    info->m = g->m;
+    info->device_bytes = g->offsets.bytes() + g->entries.bytes() + g->out_deg.bytes() + g->in_deg.bytes() +
+                         g->freq.bytes() + g->etable.bytes();
+    info->threshold_ms = g->threshold_ms;
+    return DG_OK;
+}
+
+namespace {
+__global__ void split_entries(const uint2 *entries, uint64_t m, uint32_t *nbr, uint32_t *thr) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint2 e = entries[i];
+        if (nbr) nbr[i] = e.x;
+        if (thr) thr[i] = e.y;
+    }
+}
+}  // namespace
+
+extern "C" int dg_graph_copy_csr(const dg_graph *g, uint64_t *offsets, uint32_t *neighbours, uint32_t *thresholds,
+                                 uint32_t *out_degree, uint32_t *in_degree) {
+    DG_CHECK(g, DG_ERR_ARG, "dg_graph_copy_csr: NULL graph");
+    dg::DeviceGuard guard(g->device);
+    if (offsets) DG_CUDA(cudaMemcpy(offsets, g->offsets.p, ((size_t)g->v_num + 1) * 8, cudaMemcpyDeviceToHost));
+    if (out_degree) DG_CUDA(cudaMemcpy(out_degree, g->out_deg.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToHost));
+    if (in_degree) DG_CUDA(cudaMemcpy(in_degree, g->in_deg.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToHost));
+    if ((neighbours || thresholds) && g->m) {
+        dg::DevArray<uint32_t> a, b;
+        if (neighbours) DG_CUDA(a.alloc(g->m));
+        if (thresholds) DG_CUDA(b.alloc(g->m));
+        split_entries<<<dg::sm_count(g->device) * 4, 256, 0, g->stream>>>(g->entries.p, g->m, a.p, b.p);
+        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaStreamSynchronize(g->stream));
+        if (neighbours) DG_CUDA(cudaMemcpy(neighbours, a.p, g->m * 4, cudaMemcpyDeviceToHost));
+        if (thresholds) DG_CUDA(cudaMemcpy(thresholds, b.p, g->m * 4, cudaMemcpyDeviceToHost));
+    }
+    return DG_OK;
+}
+
+extern "C" int dg_graph_copy_visits(const dg_graph *g, uint32_t *freq) {
+    DG_CHECK(g && freq, DG_ERR_ARG, "dg_graph_copy_visits: NULL argument");
+    dg::DeviceGuard guard(g->device);
+    DG_CUDA(cudaStreamSynchronize(g->stream));
+    DG_CUDA(cudaMemcpy(freq, g->freq.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToHost));
+    return DG_OK;
+}

@@ -1,0 +1,132 @@
+// Internal declarations shared by the distger CUDA sources (not part of the C ABI).
+#pragma once
+
+#include "distger.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+namespace dg {
+
+// Records `msg` as the calling thread's last error and returns `code`.
+int fail(int code, const char *fmt, ...);
+int cuda_fail(cudaError_t e, const char *what);
+void clear_error();
+
+#define DG_CUDA(call)                                              \
+    do {                                                           \
+        cudaError_t dg_e_ = (call);                                \
+        if (dg_e_ != cudaSuccess) return dg::cuda_fail(dg_e_, #call); \
+    } while (0)
+
+#define DG_CHECK(cond, code, ...)                    \
+    do {                                             \
+        if (!(cond)) return dg::fail(code, __VA_ARGS__); \
+    } while (0)
+
+// Typed device allocation that frees itself.
+template <typename T>
+struct DevArray {
+    T *p = nullptr;
+    size_t n = 0;
+    DevArray() = default;
+    DevArray(const DevArray &) = delete;
+    DevArray &operator=(const DevArray &) = delete;
+    ~DevArray() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        n = count;
+        if (count == 0) return cudaSuccess;
+        return cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
+    }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// Sets the current device for the lifetime of the guard and restores the old one.
+struct DeviceGuard {
+    int old = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&old);
+        if (dev != old) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (old >= 0 && cur != old) cudaSetDevice(old);
+    }
+};
+
+// Event pair for timing work queued on one stream.
+struct EventTimer {
+    cudaEvent_t a = nullptr, b = nullptr;
+    EventTimer() {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~EventTimer() {
+        if (a) cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+    void start(cudaStream_t s) { cudaEventRecord(a, s); }
+    void stop(cudaStream_t s) { cudaEventRecord(b, s); }
+    double ms() {
+        float t = 0.f;
+        cudaEventSynchronize(b);
+        cudaEventElapsedTime(&t, a, b);
+        return (double)t;
+    }
+};
+
+int sm_count(int device);
+
+// Exclusive prefix sum of n 32-bit counts into 64-bit offsets (out has n + 1
+// entries; out[n] = total).  Scratch is allocated internally.
+int exclusive_scan_u32_to_u64(const uint32_t *in, uint64_t *out, uint64_t n, cudaStream_t s);
+
+}  // namespace dg
+
+// Device-resident graph: int64 row offsets and 8-byte CSR entries
+// {neighbour, acceptance threshold}.
+struct dg_graph {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t v_num = 0;
+    uint64_t m = 0;
+    dg::DevArray<uint64_t> offsets;   // v_num + 1
+    dg::DevArray<uint2> entries;      // m
+    dg::DevArray<uint32_t> out_deg;   // v_num
+    dg::DevArray<uint32_t> in_deg;    // v_num
+    dg::DevArray<uint32_t> freq;      // cumulative visits, v_num
+    dg::DevArray<double> etable;      // entropy-term table
+    uint32_t etable_max_sn = 0;
+    std::vector<uint32_t> h_out_deg;
+    std::vector<double> entropy_history;
+    uint64_t visits_total = 0;        // footprints over all rounds (sum of freq)
+    double threshold_ms = 0.0;
+    ~dg_graph();
+};
+
+// One round of walks in slot layout: walk w owns vertices[w * stride, w * stride + len[w]).
+struct dg_paths {
+    dg_graph *g = nullptr;
+    int device = 0;
+    uint32_t round = 0;
+    uint32_t n_walks = 0;
+    uint32_t stride = 0;
+    dg::DevArray<uint32_t> verts;  // n_walks * stride
+    dg::DevArray<uint32_t> lens;   // n_walks
+    dg_round_info info{};
+};
+
+namespace dg {
+int ensure_entropy_table(dg_graph *g, uint32_t max_sn);
+}

@@ -1,0 +1,106 @@
+"""ctypes binding of the distger C ABI (include/distger.h, libdistger.so).
+
+The CUDA library is the only compute path: if libdistger.so is missing or
+cannot be loaded, every call raises -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libdistger.so")
+CSRC = os.path.join(PKG_DIR, "csrc")
+
+DG_OK = 0
+ERRORS = {-1: "DG_ERR_ARG", -2: "DG_ERR_IO", -3: "DG_ERR_CUDA", -4: "DG_ERR_NOMEM", -5: "DG_ERR_OVERFLOW",
+          -6: "DG_ERR_STATE"}
+
+
+class DistgerError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class GraphInfo(C.Structure):
+    _fields_ = [("v_num", C.c_uint32), ("m", C.c_uint64), ("device_bytes", C.c_uint64),
+                ("threshold_ms", C.c_double)]
+
+
+class WalkParams(C.Structure):
+    _fields_ = [("min_len", C.c_uint32), ("init_round", C.c_uint32), ("walker_num", C.c_uint32),
+                ("max_len", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class RoundInfo(C.Structure):
+    _fields_ = [("n_walks", C.c_uint32), ("footprints", C.c_uint64), ("steps", C.c_uint64),
+                ("draws", C.c_uint64), ("traces", C.c_uint64), ("max_len", C.c_uint32),
+                ("walk_ms", C.c_double), ("relative_entropy", C.c_double), ("delta_h", C.c_double)]
+
+
+class SgnsParams(C.Structure):
+    _fields_ = [("size", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("batch_size", C.c_int),
+                ("sample", C.c_float), ("alpha", C.c_float), ("iter", C.c_int), ("min_count", C.c_int),
+                ("mode", C.c_int), ("deterministic", C.c_int), ("seed", C.c_uint64),
+                ("table_size", C.c_uint64)]
+
+
+class TrainInfo(C.Structure):
+    _fields_ = [("words", C.c_uint64), ("trained", C.c_uint64), ("pairs", C.c_uint64),
+                ("train_ms", C.c_double)]
+
+
+_P = C.c_void_p
+_SIGS = {
+    "dg_last_error": ([], C.c_char_p),
+    "dg_version": ([], C.c_char_p),
+    "dg_graph_create": ([C.c_char_p, C.c_uint32, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "dg_graph_create_from_edges": ([_P, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.POINTER(_P)], C.c_int),
+    "dg_graph_free": ([_P], None),
+    "dg_graph_get_info": ([_P, C.POINTER(GraphInfo)], C.c_int),
+    "dg_graph_copy_csr": ([_P, _P, _P, _P, _P, _P], C.c_int),
+    "dg_graph_copy_visits": ([_P, _P], C.c_int),
+    "dg_walk_run_round": ([_P, C.POINTER(WalkParams), C.c_uint32, C.c_uint32, C.POINTER(_P)], C.c_int),
+    "dg_paths_get_info": ([_P, C.POINTER(RoundInfo)], C.c_int),
+    "dg_paths_copy": ([_P, _P, _P], C.c_int),
+    "dg_paths_write_text": ([_P, C.c_char_p], C.c_int),
+    "dg_paths_free": ([_P], None),
+    "dg_sgns_create": ([C.POINTER(SgnsParams), C.c_uint32, _P, C.c_int, C.POINTER(_P)], C.c_int),
+    "dg_sgns_free": ([_P], None),
+    "dg_sgns_train_paths": ([_P, _P, C.c_float, C.POINTER(TrainInfo)], C.c_int),
+    "dg_sgns_train_host": ([_P, _P, C.c_uint32, _P, C.c_float, C.POINTER(TrainInfo)], C.c_int),
+    "dg_sgns_copy_embedding": ([_P, _P, _P, C.POINTER(C.c_uint32)], C.c_int),
+    "dg_sgns_copy_output": ([_P, _P], C.c_int),
+    "dg_sgns_set_rows": ([_P, _P, _P], C.c_int),
+    "dg_sgns_write_embedding": ([_P, C.c_char_p], C.c_int),
+}
+
+_lib = None
+
+
+def build() -> None:
+    """Compile the CUDA sources for sm_100a into gdistger-re_b200/libdistger.so."""
+    subprocess.run(["make", "-s", "-C", CSRC], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is not built; run distger.build() (nvcc, sm_100a)")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in _SIGS.items():
+            fn = getattr(L, name, None)
+            if fn is None:
+                continue
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != DG_OK:
+        raise DistgerError(rc, lib().dg_last_error().decode(errors="replace"))

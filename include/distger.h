@@ -1,0 +1,188 @@
+/*
+ * distger: B200 (sm_100a) implementation of DistGER's embedding hot path --
+ * the information-oriented random walk and the skip-gram negative-sampling
+ * (SGNS) trainer -- behind a plain C ABI.
+ *
+ * Conventions: every entry point returns 0 (DG_OK) or a negative DG_ERR_* code
+ * and never exits the process; dg_last_error() gives the message of the calling
+ * thread's last failure.  Handles own their device memory and one CUDA stream;
+ * a handle is not thread-safe.  Host buffers are plain pointers with sizes.
+ *
+ * Reference interfaces replaced (paths within the reference project):
+ *  - graph load + CSR:  GraphEngine::load_graph, include/graph.hpp:642-824,
+ *                       read_graph, include/storage.hpp:15-37
+ *  - walk rounds:       WalkEngine::random_walk / internal_random_walk,
+ *                       include/walk.hpp:512, 609-782; internal_walk_epoch 790-1043
+ *  - walk output:       PathCollector::assemble_path + PathSet::dump,
+ *                       include/path.hpp:175-551, 67-119
+ *  - SGNS trainer:      train_corpus_cuda / TrainModel / TrainModelThread,
+ *                       src/word2vec.cu:1429, 1246, 952; dsgl(), include/dsgl.hpp:1464
+ *  - LR schedule:       include/lr_scheduler.hpp:5-74
+ */
+#ifndef DISTGER_H
+#define DISTGER_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define DG_API __attribute__((visibility("default")))
+#else
+#define DG_API
+#endif
+
+#define DG_OK 0
+#define DG_ERR_ARG -1        /* invalid argument or size */
+#define DG_ERR_IO -2         /* file missing, unreadable or malformed */
+#define DG_ERR_CUDA -3       /* CUDA runtime error (message has the CUDA string) */
+#define DG_ERR_NOMEM -4      /* host or device allocation failed */
+#define DG_ERR_OVERFLOW -5   /* a walk outgrew its arena slot; rerun with larger max_len */
+#define DG_ERR_STATE -6      /* call out of order (e.g. no paths yet) */
+
+typedef struct dg_graph dg_graph;
+typedef struct dg_paths dg_paths;
+typedef struct dg_sgns dg_sgns;
+
+/* Message of the calling thread's last failed call ("" if none). */
+DG_API const char *dg_last_error(void);
+
+/* Library build identity: "distger <version> sm_100a". */
+DG_API const char *dg_version(void);
+
+/* ------------------------------------------------------------------ graph */
+
+/* Loads packed 12-byte {u32 src, u32 dst, f32 data} records (storage.hpp:15-37,
+ * type.hpp:67-91), optionally makes them undirected by emitting each record and
+ * its transpose (graph.hpp:671-686), and builds the device CSR: int64 row
+ * offsets, 8-byte entries {u32 neighbour, u32 acceptance threshold}.  Vertex ids
+ * >= v_num and edge data that is NaN or outside int range are DG_ERR_ARG;
+ * a file whose size is not a multiple of 12 is DG_ERR_IO. */
+DG_API int dg_graph_create(const char *edge_path, uint32_t v_num, int undirected, int device, dg_graph **out);
+
+/* Same from host records already in memory (n_edges records of 12 bytes). */
+DG_API int dg_graph_create_from_edges(const void *edges, uint64_t n_edges, uint32_t v_num, int undirected,
+                               int device, dg_graph **out);
+
+DG_API void dg_graph_free(dg_graph *g);
+
+typedef struct {
+    uint32_t v_num;
+    uint64_t m;               /* directed CSR entries */
+    uint64_t device_bytes;    /* device memory held by the graph */
+    double threshold_ms;      /* acceptance-threshold kernel time */
+} dg_graph_info;
+DG_API int dg_graph_get_info(const dg_graph *g, dg_graph_info *info);
+
+/* Copies the CSR to host buffers (each may be NULL): offsets[v_num+1],
+ * neighbours[m], thresholds[m], out_degree[v_num], in_degree[v_num]. */
+DG_API int dg_graph_copy_csr(const dg_graph *g, uint64_t *offsets, uint32_t *neighbours, uint32_t *thresholds,
+                      uint32_t *out_degree, uint32_t *in_degree);
+
+/* ------------------------------------------------------------------ walks */
+
+typedef struct {
+    uint32_t min_len;     /* --min_L: no termination test until step > min_len (walk.hpp:404, 868) */
+    uint32_t init_round;  /* --min_R: round 1 runs walker_num * init_round walkers (walk.hpp:614) */
+    uint32_t walker_num;  /* -w */
+    uint32_t max_len;     /* arena slot, in footprints; 0 = 64.  Longer walks are DG_ERR_OVERFLOW */
+    uint64_t seed;        /* Philox key for seeded replay */
+} dg_walk_params;
+
+typedef struct {
+    uint32_t n_walks;
+    uint64_t footprints;  /* all footprints, start vertices included */
+    uint64_t steps;       /* footprints with step >= 1 (the reference's p_step counter) */
+    uint64_t draws;       /* candidate draws */
+    uint64_t traces;      /* rejected candidates (walk.hpp trace_num) */
+    uint32_t max_len;     /* longest walk, footprints */
+    double walk_ms;       /* walk kernel time (CUDA events) */
+    double relative_entropy; /* after this round's visits are counted (walk.hpp:694-725) */
+    double delta_h;          /* change vs the previous round (walk.hpp:727-728) */
+} dg_round_info;
+
+/* Runs one round: walkers 0..n-1 start at id % v_num (walk.hpp:501-509) with
+ * n = walker_num * init_round for round 1, walker_num otherwise (n_walkers != 0
+ * overrides).  The walks stay on the device in *out; the graph's cumulative
+ * visit frequencies (context_map_freq, walk.hpp:645, 688) are updated.
+ * Seeded replay: identical (seed, round, walker) give identical walks. */
+DG_API int dg_walk_run_round(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_walkers,
+                      dg_paths **out);
+
+DG_API int dg_paths_get_info(const dg_paths *paths, dg_round_info *info);
+
+/* Copies walks in walker order: offsets[n_walks+1] (footprint offsets) and
+ * vertices[footprints] (either may be NULL). */
+DG_API int dg_paths_copy(const dg_paths *paths, uint64_t *offsets, uint32_t *vertices);
+
+/* Writes the walk file: per walk " %u" per vertex then "\n" (path.hpp:92,108).
+ * The text is formatted on the device. */
+DG_API int dg_paths_write_text(const dg_paths *paths, const char *file_path);
+
+DG_API void dg_paths_free(dg_paths *paths);
+
+/* Cumulative visit frequency per vertex over all rounds run on g. */
+DG_API int dg_graph_copy_visits(const dg_graph *g, uint32_t *freq);
+
+/* ------------------------------------------------------------------- SGNS */
+
+enum {
+    DG_SGNS_PLAIN = 0,      /* word2vec.cu skip_gram_kernel semantics: FP32 rows, per-pair negatives, Hogwild */
+    DG_SGNS_MINIBATCH = 1,  /* dsgl.hpp Train_SGNS_MPI semantics: shared negatives, BF16 rows, FP32 accumulation */
+};
+
+typedef struct {
+    int size;          /* -size: embedding dimension (multiple of 32, <= 512) */
+    int window;        /* -window */
+    int negative;      /* -negative */
+    int batch_size;    /* -batch-size (minibatch mode; dsgl overrides it with 2*window+1, dsgl.hpp:832) */
+    float sample;      /* -sample */
+    float alpha;       /* -alpha */
+    int iter;          /* -iter: passes over each round's walks */
+    int min_count;     /* -min-count */
+    int mode;          /* DG_SGNS_* */
+    int deterministic; /* 1: one warp trains everything in order (tests, replay) */
+    uint64_t seed;
+    uint64_t table_size; /* unigram table slots; 0 = 1e8 (word2vec.cu:66) */
+} dg_sgns_params;
+
+/* Vocabulary from per-vertex counts (word2vec.cu:791-809 uses in+out degree,
+ * dsgl.hpp:307-352 uses walk visit counts): sorted by count, descending, ties by
+ * vertex id; counts < min_count dropped except the first (word2vec.cu:632-659).
+ * Input rows initialised with word2vec's LCG (word2vec.cu:870-873), output rows
+ * zero; unigram^0.75 table (word2vec.cu:537-556). */
+DG_API int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uint32_t *vertex_counts, int device,
+                   dg_sgns **out);
+DG_API void dg_sgns_free(dg_sgns *s);
+
+typedef struct {
+    uint64_t words;      /* tokens consumed, subsampled ones included (word2vec.cu word_count) */
+    uint64_t trained;    /* tokens kept after subsampling */
+    uint64_t pairs;      /* (centre, context) pairs */
+    double train_ms;     /* SGNS kernel time */
+} dg_train_info;
+
+/* One pass (x iter) over a round's walks with learning rate alpha (alpha <= 0:
+ * the params' alpha). */
+DG_API int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alpha, dg_train_info *info);
+
+/* Same over host walks in walker order (offsets[n_walks+1], vertices[...]). */
+DG_API int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t n_walks, const uint32_t *vertices,
+                       float alpha, dg_train_info *info);
+
+/* Input rows (the embedding) as FP32, in vocabulary order; vocab_ids[rows]
+ * gives the vertex of each row.  Either pointer may be NULL. */
+DG_API int dg_sgns_copy_embedding(const dg_sgns *s, float *rows, uint32_t *vocab_ids, uint32_t *n_rows);
+DG_API int dg_sgns_copy_output(const dg_sgns *s, float *rows);
+DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *output_rows);
+
+/* Embedding text: "%lld %lld\n" header then per row "%u " + size x "%lf " + "\n"
+ * (word2vec.cu:1353-1362). */
+DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -217,6 +217,26 @@ int dgo_walk_round(const dgo_csr *g, const dgo_walk_params *p, uint32_t round, u
     return 0;
 }
 
+/* The walks of selected walker ids only (same per-walker semantics; Philox mode),
+ * for spot checks of full-size rounds. */
+int dgo_walk_ids(const dgo_csr *g, const dgo_walk_params *p, uint32_t round, const uint32_t *ids, uint32_t n_ids,
+                 dgo_paths *out, dgo_walk_stats *stats) {
+    memset(out, 0, sizeof(*out));
+    if (g->v_num == 0 || p->rng_mode != DGO_RNG_PHILOX) return -1;
+    dgo_vec v = {0, 0, 0};
+    out->offsets = (uint64_t *)malloc(((size_t)n_ids + 1) * sizeof(uint64_t));
+    if (!out->offsets) return -2;
+    out->offsets[0] = 0;
+    for (uint32_t i = 0; i < n_ids; i++) {
+        if (walk_one(g, p, round, ids[i], &v, stats)) { free(v.v); return -2; }
+        out->offsets[i + 1] = v.n;
+    }
+    out->n_walks = n_ids;
+    out->total = v.n;
+    out->verts = v.v ? v.v : (uint32_t *)malloc(4);
+    return 0;
+}
+
 void dgo_paths_free(dgo_paths *p) {
     free(p->offsets); free(p->verts);
     memset(p, 0, sizeof(*p));
@@ -281,4 +301,11 @@ void dgo_entropy_table(uint32_t max_sn, double *out) {
     for (uint32_t s = 1; s <= max_sn; s++)
         for (uint32_t f = 0; f <= s; f++)
             out[(uint64_t)s * (s + 1) / 2 + f - 1] = entropy_term((double)s, (double)f);
+}
+
+/* Known-answer hook for the Philox restatement. */
+void dgo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    dgo_u32x4 c = {{ctr[0], ctr[1], ctr[2], ctr[3]}};
+    dgo_u32x4 r = dgo_philox4x32_10(c, key[0], key[1]);
+    for (int i = 0; i < 4; i++) out[i] = r.v[i];
 }

@@ -82,6 +82,10 @@ int dgo_walk_round(const dgo_csr *g, const dgo_walk_params *p, uint32_t round, u
                    dgo_paths *out, dgo_walk_stats *stats);
 void dgo_paths_free(dgo_paths *p);
 
+/* Walks of the listed walker ids of `round` (Philox mode only). */
+int dgo_walk_ids(const dgo_csr *g, const dgo_walk_params *p, uint32_t round, const uint32_t *ids, uint32_t n_ids,
+                 dgo_paths *out, dgo_walk_stats *stats);
+
 /* Writes one walk per line as " %u" per vertex then "\n" (path.hpp:67-119). */
 int dgo_write_walks(const char *path, const dgo_paths *p);
 
@@ -98,6 +102,9 @@ void dgo_thresholds(const dgo_csr *g, uint32_t *thr);
  * Sn*(Sn+1)/2 + fi - 1. */
 void dgo_entropy_table(uint32_t max_sn, double *out);
 uint64_t dgo_entropy_table_size(uint32_t max_sn);
+
+/* Philox4x32-10 block (known-answer tests). */
+void dgo_philox(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 
 /* The reference's candidate / acceptance streams for the pin test:
  * std::mt19937(seed) + std::uniform_int_distribution<uint32_t>(0, degree-1)

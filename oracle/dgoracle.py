@@ -81,6 +81,9 @@ def lib():
         L.dgo_stream_new.argtypes = [C.c_uint32]
         L.dgo_stream_new.restype = C.c_void_p
         L.dgo_stream_free.argtypes = [C.c_void_p]
+        L.dgo_philox.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dgo_walk_ids.argtypes = [C.POINTER(_Csr), C.POINTER(_WalkParams), C.c_uint32, C.c_void_p, C.c_uint32,
+                                   C.POINTER(_Paths), C.POINTER(WalkStats)]
         _lib = L
     return _lib
 
@@ -157,6 +160,23 @@ def walk_rounds(csr: Csr, walker_num: int, min_len: int = 20, init_round: int = 
     return out, stats
 
 
+def walk_ids(csr: Csr, ids, round_index: int, min_len: int = 20, seed: int = 0):
+    """Philox-mode walks of the given walker ids of one round: (offsets, verts)."""
+    L = lib()
+    ids = np.ascontiguousarray(ids, dtype=np.uint32)
+    p = _WalkParams(min_len=min_len, init_round=1, walker_num=1, rounds=round_index, seed=seed, rng_mode=0)
+    paths = _Paths()
+    stats = WalkStats()
+    rc = L.dgo_walk_ids(C.byref(csr._c), C.byref(p), round_index, ids.ctypes.data, ids.size, C.byref(paths),
+                        C.byref(stats))
+    if rc:
+        raise RuntimeError(f"dgo_walk_ids failed ({rc})")
+    offs = np.ctypeslib.as_array(paths.offsets, shape=(ids.size + 1,)).copy()
+    verts = _u32(paths.verts, paths.total)
+    L.dgo_paths_free(C.byref(paths))
+    return offs, verts
+
+
 def walk_text(offsets: np.ndarray, verts: np.ndarray) -> bytes:
     """Walk file bytes: " %u" per vertex, "\\n" per walk (path.hpp:92,108)."""
     parts = []
@@ -170,6 +190,24 @@ def relative_entropy(out_deg: np.ndarray, freq: np.ndarray) -> float:
     out_deg = np.ascontiguousarray(out_deg, dtype=np.uint32)
     freq = np.ascontiguousarray(freq, dtype=np.uint32)
     return lib().dgo_relative_entropy(out_deg.ctypes.data, freq.ctypes.data, out_deg.size)
+
+
+def philox(ctr, key) -> list:
+    c = np.ascontiguousarray(ctr, dtype=np.uint32)
+    k = np.ascontiguousarray(key, dtype=np.uint32)
+    out = np.zeros(4, dtype=np.uint32)
+    lib().dgo_philox(c.ctypes.data, k.ctypes.data, out.ctypes.data)
+    return [int(x) for x in out]
+
+
+def load_golden(path: str):
+    z = np.load(path)
+    rounds = []
+    r = 1
+    while f"offsets_{r}" in z:
+        rounds.append((z[f"offsets_{r}"], z[f"verts_{r}"]))
+        r += 1
+    return rounds, z["abs_delta_h"], z["meta"]
 
 
 def entropy_table(max_sn: int) -> np.ndarray:

@@ -1,0 +1,667 @@
+// Skip-gram negative-sampling trainer over device-resident walks.
+//
+//  * plain form (DG_SGNS_PLAIN): the update rule of word2vec.cu skip_gram_kernel
+//    (word2vec.cu:305-399) on FP32 rows; one warp per walk, each lane owning
+//    size/32 contiguous dimensions, dot products by warp shuffles, Hogwild
+//    vector atomics between warps;
+//  * minibatch form (DG_SGNS_MINIBATCH): dsgl.hpp Train_SGNS_MPI semantics
+//    (dsgl.hpp:783-1407), see dg_sgns_mb.cu.
+#include "dg_sgns.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <thread>
+
+namespace dgs {
+
+// ------------------------------------------------------------------ host prep
+
+// ReadVocabFromDegree + SortVocab (word2vec.cu:791-809, 632-659).
+void build_vocab(const uint32_t *counts, uint32_t v_num, int min_count, std::vector<uint32_t> &ids,
+                 std::vector<uint32_t> &cn, std::vector<int32_t> &v2w, uint64_t &train_words) {
+    std::vector<uint32_t> order(v_num);
+    for (uint32_t v = 0; v < v_num; v++) order[v] = v;
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return counts[a] > counts[b]; });
+    v2w.assign(v_num, -1);
+    ids.clear();
+    cn.clear();
+    train_words = 0;
+    for (uint32_t i = 0; i < v_num; i++) {
+        const uint32_t v = order[i];
+        if ((int64_t)counts[v] < min_count && i != 0) continue;
+        v2w[v] = (int32_t)ids.size();
+        ids.push_back(v);
+        cn.push_back(counts[v]);
+        train_words += counts[v];
+    }
+}
+
+// InitUnigramTable (word2vec.cu:537-556), power 0.75.
+void unigram_table(const std::vector<uint32_t> &cn, uint64_t table_size, std::vector<int32_t> &table) {
+    const uint32_t vs = (uint32_t)cn.size();
+    table.resize(table_size);
+    double train_words_pow = 0;
+    for (uint32_t a = 0; a < vs; a++) train_words_pow += std::pow((double)cn[a], 0.75);
+    uint32_t i = 0;
+    double d1 = std::pow((double)cn[0], 0.75) / train_words_pow;
+    for (uint64_t a = 0; a < table_size; a++) {
+        table[a] = (int32_t)i;
+        if (a / (double)table_size > d1) {
+            i++;
+            if (i < vs) d1 += std::pow((double)cn[i], 0.75) / train_words_pow;
+        }
+        if (i >= vs) i = vs - 1;
+    }
+}
+
+// Subsampling: a token of word w is kept iff its 16 random bits are < thr[w]
+// (discard iff ran < u / 65536, word2vec.cu:1022-1026 or dsgl.hpp:931-937).
+void keep_thresholds(const std::vector<uint32_t> &cn, float sample, uint64_t train_words, bool dsgl_form,
+                     std::vector<uint32_t> &thr) {
+    thr.resize(cn.size());
+    for (size_t w = 0; w < cn.size(); w++) {
+        if (!(sample > 0)) {
+            thr[w] = 65536;
+            continue;
+        }
+        const float sT = sample * (float)train_words;
+        float ran;
+        if (dsgl_form) {
+            const float ratio = sT / (float)cn[w];
+            ran = std::sqrt(ratio) + ratio;
+        } else {
+            ran = (std::sqrt((float)cn[w] / sT) + 1) * sT / (float)cn[w];
+        }
+        uint32_t k;
+        if (ran != ran || ran < 0.0f) k = 0;
+        else if (ran >= 1.0f) k = 65536;
+        else k = std::min<uint32_t>(65536, (uint32_t)std::floor(ran * 65536.0f) + 1);
+        thr[w] = k;
+    }
+}
+
+// expTable (word2vec.cu:1569-1573).
+void exp_table(std::vector<float> &t) {
+    t.assign(kExpTableSize + 1, 0.0f);
+    for (int i = 0; i < kExpTableSize; i++) {
+        t[i] = std::exp((i / (float)kExpTableSize * 2 - 1) * kMaxExp);
+        t[i] = t[i] / (t[i] + 1);
+    }
+}
+
+// -------------------------------------------------------------- device init
+
+// word2vec's LCG (word2vec.cu:870-873) evaluated at element k directly: the
+// state after k + 1 steps from 1, by composing the affine map x -> A x + C.
+__device__ __forceinline__ unsigned long long lcg_state(unsigned long long k) {
+    unsigned long long ra = 1, rc = 0;                      // identity
+    unsigned long long ba = 25214903917ULL, bc = 11ULL;     // one step
+    unsigned long long n = k + 1;
+    while (n) {
+        if (n & 1) {
+            rc = ra * bc + rc;
+            ra = ra * ba;
+        }
+        bc = ba * bc + bc;
+        ba = ba * ba;
+        n >>= 1;
+    }
+    return ra * 1ULL + rc;
+}
+
+__global__ void init_rows_f32(float *rows, uint64_t n, int d) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long x = lcg_state(k);
+        rows[k] = (((x & 0xFFFF) / (float)65536) - 0.5f) / d;
+    }
+}
+
+__global__ void init_rows_bf16(__nv_bfloat16 *rows, float *master, uint64_t n, uint64_t n_master, int d) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long x = lcg_state(k);
+        const float v = (((x & 0xFFFF) / (float)65536) - 0.5f) / d;
+        rows[k] = __float2bfloat16_rn(v);
+        if (k < n_master) master[k] = v;
+    }
+}
+
+// ------------------------------------------------------------ plain kernel
+
+template <int VEC>
+struct RowVec {
+    float v[VEC];
+};
+
+template <int VEC>
+__device__ __forceinline__ void load_row(const float *p, RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4) {
+            const float4 t = __ldcg(reinterpret_cast<const float4 *>(p + i));
+            r.v[i] = t.x; r.v[i + 1] = t.y; r.v[i + 2] = t.z; r.v[i + 3] = t.w;
+        }
+    } else if constexpr (VEC == 2) {
+        const float2 t = __ldcg(reinterpret_cast<const float2 *>(p));
+        r.v[0] = t.x; r.v[1] = t.y;
+    } else {
+        r.v[0] = __ldcg(p);
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void store_row(float *p, const RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            __stcg(reinterpret_cast<float4 *>(p + i), make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]));
+    } else if constexpr (VEC == 2) {
+        __stcg(reinterpret_cast<float2 *>(p), make_float2(r.v[0], r.v[1]));
+    } else {
+        __stcg(p, r.v[0]);
+    }
+}
+
+// p[i] += r[i] with 16-byte vector atomics (sm_90+).
+template <int VEC>
+__device__ __forceinline__ void add_row(float *p, const RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            atomicAdd(reinterpret_cast<float4 *>(p + i), make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]));
+    } else if constexpr (VEC == 2) {
+        atomicAdd(reinterpret_cast<float2 *>(p), make_float2(r.v[0], r.v[1]));
+    } else {
+        atomicAdd(p, r.v[0]);
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ float warp_dot(const RowVec<VEC> &a, const RowVec<VEC> &b) {
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < VEC; i++) s = fmaf(a.v[i], b.v[i], s);
+#pragma unroll
+    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return __shfl_sync(0xffffffffu, s, 0);  // one value for every lane
+}
+
+// g = (label - sigmoid(f)) * alpha through expTable (word2vec.cu:383-388), with
+// the reference's integer-division index scale (EXP_TABLE_SIZE / MAX_EXP / 2 = 83).
+__device__ __forceinline__ float sg_grad(float f, int label, const float *exp_table, float alpha) {
+    if (f > kMaxExp) return (label - 1) * alpha;
+    if (f < -kMaxExp) return label * alpha;
+    return (label - exp_table[(int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2))]) * alpha;
+}
+
+__device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
+    return philox4x32_10(make_uint4(c0, c1, c2, c3), k0, k1);
+}
+
+// Builds the walk's sentence in shared memory: vocabulary lookup + subsampling
+// (word2vec.cu:1011-1029 with a Philox draw in place of rand()).  Returns its length.
+__device__ __forceinline__ uint32_t warp_sentence(const WalkSet &ws, uint32_t walk, const SgnsArgs &a, int32_t *sen,
+                                                  uint32_t &words) {
+    const uint32_t lane = threadIdx.x & 31;
+    uint64_t begin;
+    uint32_t len;
+    ws.range(walk, begin, len);
+    if (len > kMaxSentence) len = kMaxSentence;
+    words = len;
+    uint32_t n = 0;
+    for (uint32_t base = 0; base < len; base += 32) {
+        const uint32_t i = base + lane;
+        bool keep = false;
+        int32_t w = -1;
+        if (i < len) {
+            w = a.v2w[ws.verts[begin + i]];
+            if (w >= 0) {
+                const uint32_t u = philox(i, ws.ids ? ws.ids[walk] : walk + ws.id_base, a.pass, kSubTag, a.seed_lo,
+                                          a.seed_hi).x & 0xFFFFu;
+                keep = u < a.keep_thr[w];
+            }
+        }
+        const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+        if (keep) sen[n + __popc(mask & ((1u << lane) - 1))] = w;
+        n += __popc(mask);
+    }
+    __syncwarp();
+    return n;
+}
+
+template <int VEC>
+__global__ void __launch_bounds__(kPlainThreads) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[kPlainThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    const int d = 32 * VEC;
+    const float alpha = a.alpha;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % (uint32_t)a.window;
+            float *pos_row = a.syn1 + (size_t)word * d + lane * VEC;
+            RowVec<VEC> pos, pos0;
+            load_row<VEC>(pos_row, pos);
+            pos0 = pos;
+            for (uint32_t s = b; s < (uint32_t)(2 * a.window + 1) - b; s++) {
+                if (s == (uint32_t)a.window) continue;
+                const int64_t c = (int64_t)p - a.window + s;
+                if (c < 0 || c >= (int64_t)n) continue;
+                const int32_t last = sen[c];
+                float *l1p = a.syn0 + (size_t)last * d + lane * VEC;
+                RowVec<VEC> l1, e;
+                load_row<VEC>(l1p, l1);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
+                n_pairs++;
+                // Positive target: the centre word (row kept in registers for this centre).
+                {
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                    }
+                }
+                if (a.vocab_size > 1) {
+                    uint4 blk = make_uint4(0, 0, 0, 0);
+                    for (int j = 1; j <= a.negative; j++) {
+                        if (((j - 1) & 3) == 0)
+                            blk = philox(p * (2 * a.window + 1) + s, wid, a.pass, kNegTag + (uint32_t)((j - 1) >> 2),
+                                         a.seed_lo, a.seed_hi);
+                        const uint32_t q = (j - 1) & 3;
+                        const uint32_t r = q == 0 ? blk.x : q == 1 ? blk.y : q == 2 ? blk.z : blk.w;
+                        int32_t target = a.table[r % a.table_size];
+                        if (target == 0) target = (int32_t)((r >> 8) % (a.vocab_size - 1) + 1);  // word2vec.cu:367
+                        if (target == word) continue;
+                        float *l2p = a.syn1 + (size_t)target * d + lane * VEC;
+                        RowVec<VEC> l2, upd;
+                        load_row<VEC>(l2p, l2);
+                        const float g = sg_grad(warp_dot<VEC>(l1, l2), 0, a.exp_table, alpha);
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) {
+                            e.v[i] = fmaf(g, l2.v[i], e.v[i]);
+                            upd.v[i] = __fmul_rn(g, l1.v[i]);  // rounded product, never fused
+                        }
+                        if (a.deterministic) {
+#pragma unroll
+                            for (int i = 0; i < VEC; i++) l2.v[i] += upd.v[i];
+                            store_row<VEC>(l2p, l2);
+                        } else {
+                            add_row<VEC>(l2p, upd);
+                        }
+                    }
+                }
+                if (a.deterministic) {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
+                    store_row<VEC>(l1p, l1);
+                } else {
+                    add_row<VEC>(l1p, e);
+                }
+            }
+            if (a.deterministic) {
+                store_row<VEC>(pos_row, pos);
+            } else {
+#pragma unroll
+                for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
+                add_row<VEC>(pos_row, pos);
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
+int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    const int vec = s->p.size / 32;
+    int blocks = 1, threads = 32;
+    auto occ = [&](auto kern) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kPlainThreads, 0);
+        return std::max(per_sm, 1);
+    };
+    if (!s->p.deterministic) threads = kPlainThreads;
+    switch (vec) {
+#define DG_PLAIN_CASE(V)                                                                       \
+    case V:                                                                                    \
+        if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_kernel<V>); \
+        sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                        \
+        break;
+        DG_PLAIN_CASE(1)
+        DG_PLAIN_CASE(2)
+        DG_PLAIN_CASE(4)
+        DG_PLAIN_CASE(8)
+        DG_PLAIN_CASE(16)
+#undef DG_PLAIN_CASE
+    default:
+        return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
+    }
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
+// ----------------------------------------------------------------- output
+
+__global__ void rows_to_f32(const __nv_bfloat16 *rows, const float *master, uint64_t n, uint64_t n_master, float *out) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        out[k] = k < n_master ? master[k] : __bfloat162float(rows[k]);
+}
+
+__global__ void rows_from_f32(const float *in, uint64_t n, uint64_t n_master, __nv_bfloat16 *rows, float *master) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
+        rows[k] = __float2bfloat16_rn(in[k]);
+        if (k < n_master) master[k] = in[k];
+    }
+}
+
+int copy_rows(const dg_sgns *s, bool input, float *host) {
+    const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
+    if (s->p.mode == DG_SGNS_PLAIN) {
+        DG_CUDA(cudaMemcpyAsync(host, input ? s->syn0.p : s->syn1.p, n * 4, cudaMemcpyDeviceToHost, s->stream));
+        DG_CUDA(cudaStreamSynchronize(s->stream));
+        return DG_OK;
+    }
+    dg::DevArray<float> tmp;
+    DG_CUDA(tmp.alloc(n));
+    rows_to_f32<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(input ? s->in_bf.p : s->out_bf.p,
+                                                                     input ? s->in_master.p : s->out_master.p, n,
+                                                                     (uint64_t)s->n_master * s->p.size, tmp.p);
+    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaMemcpyAsync(host, tmp.p, n * 4, cudaMemcpyDeviceToHost, s->stream));
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    return DG_OK;
+}
+
+}  // namespace dgs
+
+dg_sgns::~dg_sgns() {
+    if (stream) {
+        dg::DeviceGuard guard(device);
+        cudaStreamSynchronize(stream);
+        v2w.release(); keep_thr.release(); table.release(); exp_table.release();
+        syn0.release(); syn1.release(); in_bf.release(); out_bf.release(); in_master.release(); out_master.release();
+        scratch.release(); queue.release(); stats.release();
+        cudaStreamDestroy(stream);
+    }
+}
+
+extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uint32_t *vertex_counts, int device,
+                              dg_sgns **out) {
+    using namespace dgs;
+    DG_CHECK(p && vertex_counts && out, DG_ERR_ARG, "dg_sgns_create: NULL argument");
+    *out = nullptr;
+    DG_CHECK(v_num > 0, DG_ERR_ARG, "dg_sgns_create: v_num must be positive");
+    DG_CHECK(p->size >= 32 && p->size <= 512 && p->size % 32 == 0 && ((p->size / 32) & (p->size / 32 - 1)) == 0,
+             DG_ERR_ARG, "size %d not supported (32, 64, 128, 256 or 512)", p->size);
+    DG_CHECK(p->window >= 1 && p->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", p->window);
+    DG_CHECK(p->negative >= 0 && p->negative <= 64, DG_ERR_ARG, "negative %d out of range [0, 64]", p->negative);
+    DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH, DG_ERR_ARG, "unknown mode %d", p->mode);
+    DG_CHECK(p->iter >= 1, DG_ERR_ARG, "iter must be >= 1");
+    int n_dev = 0;
+    DG_CUDA(cudaGetDeviceCount(&n_dev));
+    DG_CHECK(device >= 0 && device < n_dev, DG_ERR_ARG, "device %d out of range (%d)", device, n_dev);
+
+    std::unique_ptr<dg_sgns> s(new dg_sgns());
+    s->device = device;
+    s->p = *p;
+    if (s->p.table_size == 0) s->p.table_size = kDefaultTableSize;
+    DG_CHECK(s->p.table_size < (1ull << 32), DG_ERR_ARG, "table_size must be < 2^32");
+    s->v_num = v_num;
+    build_vocab(vertex_counts, v_num, p->min_count, s->vocab_ids, s->vocab_cn, s->h_v2w, s->train_words);
+    s->vocab_size = (uint32_t)s->vocab_ids.size();
+    std::vector<uint32_t> thr;
+    keep_thresholds(s->vocab_cn, p->sample, s->train_words, p->mode == DG_SGNS_MINIBATCH, thr);
+    std::vector<int32_t> table;
+    unigram_table(s->vocab_cn, s->p.table_size, table);
+    std::vector<float> et;
+    exp_table(et);
+
+    dg::DeviceGuard guard(device);
+    DG_CUDA(cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    DG_CUDA(s->v2w.alloc(v_num));
+    DG_CUDA(s->keep_thr.alloc(s->vocab_size));
+    DG_CUDA(s->table.alloc(s->p.table_size));
+    DG_CUDA(s->exp_table.alloc(et.size()));
+    DG_CUDA(s->queue.alloc(1));
+    DG_CUDA(s->stats.alloc(4));
+    DG_CUDA(cudaMemcpyAsync(s->v2w.p, s->h_v2w.data(), (size_t)v_num * 4, cudaMemcpyHostToDevice, s->stream));
+    DG_CUDA(cudaMemcpyAsync(s->keep_thr.p, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    DG_CUDA(cudaMemcpyAsync(s->table.p, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    DG_CUDA(cudaMemcpyAsync(s->exp_table.p, et.data(), et.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    const uint64_t n = (uint64_t)s->vocab_size * p->size;
+    const int blocks = dg::sm_count(device) * 8;
+    if (p->mode == DG_SGNS_PLAIN) {
+        DG_CUDA(s->syn0.alloc(n));
+        DG_CUDA(s->syn1.alloc(n));
+        init_rows_f32<<<blocks, 256, 0, s->stream>>>(s->syn0.p, n, p->size);
+        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaMemsetAsync(s->syn1.p, 0, n * 4, s->stream));
+    } else {
+        s->n_master = std::min<uint32_t>(s->vocab_size, p->master_rows ? p->master_rows : kMasterRows);
+        const uint64_t nm = (uint64_t)s->n_master * p->size;
+        DG_CUDA(s->in_bf.alloc(n));
+        DG_CUDA(s->out_bf.alloc(n));
+        DG_CUDA(s->in_master.alloc(nm));
+        DG_CUDA(s->out_master.alloc(nm));
+        init_rows_bf16<<<blocks, 256, 0, s->stream>>>(s->in_bf.p, s->in_master.p, n, nm, p->size);
+        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaMemsetAsync(s->out_bf.p, 0, n * 2, s->stream));
+        DG_CUDA(cudaMemsetAsync(s->out_master.p, 0, nm * 4, s->stream));
+    }
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    *out = s.release();
+    return DG_OK;
+}
+
+extern "C" void dg_sgns_free(dg_sgns *s) { delete s; }
+
+static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train_info *info) {
+    using namespace dgs;
+    dg::DeviceGuard guard(s->device);
+    SgnsArgs a{};
+    a.v2w = s->v2w.p;
+    a.keep_thr = s->keep_thr.p;
+    a.table = s->table.p;
+    a.exp_table = s->exp_table.p;
+    a.syn0 = s->syn0.p;
+    a.syn1 = s->syn1.p;
+    a.in_bf = s->in_bf.p;
+    a.out_bf = s->out_bf.p;
+    a.in_master = s->in_master.p;
+    a.out_master = s->out_master.p;
+    a.n_master = s->n_master;
+    a.queue = s->queue.p;
+    a.stats = s->stats.p;
+    a.table_size = s->p.table_size;
+    a.vocab_size = s->vocab_size;
+    a.window = s->p.window;
+    a.negative = s->p.negative;
+    a.d = s->p.size;
+    a.alpha = alpha > 0 ? alpha : s->p.alpha;
+    a.seed_lo = (uint32_t)s->p.seed;
+    a.seed_hi = (uint32_t)(s->p.seed >> 32);
+    a.deterministic = s->p.deterministic;
+    a.train_words = s->train_words;
+    DG_CUDA(cudaMemsetAsync(s->stats.p, 0, 4 * sizeof(unsigned long long), s->stream));
+    dg::EventTimer t;
+    t.start(s->stream);
+    for (int it = 0; it < s->p.iter; it++) {
+        a.pass = s->pass++;
+        DG_CUDA(cudaMemsetAsync(s->queue.p, 0, sizeof(uint32_t), s->stream));
+        int rc = s->p.mode == DG_SGNS_PLAIN ? launch_plain(s, a, ws) : launch_minibatch(s, a, ws);
+        if (rc) return rc;
+    }
+    t.stop(s->stream);
+    unsigned long long st[4];
+    DG_CUDA(cudaMemcpyAsync(st, s->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    if (info) {
+        info->words = st[0];
+        info->trained = st[1];
+        info->pairs = st[2];
+        info->train_ms = t.ms();
+    }
+    return DG_OK;
+}
+
+extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alpha, dg_train_info *info) {
+    DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_train_paths: NULL argument");
+    DG_CHECK(paths->device == s->device, DG_ERR_ARG, "paths and trainer live on different devices");
+    DG_CHECK(paths->g->v_num <= s->v_num, DG_ERR_ARG, "walks reference vertices beyond the vocabulary's v_num");
+    dgs::WalkSet ws{};
+    ws.verts = paths->verts.p;
+    ws.lens = paths->lens.p;
+    ws.stride = paths->stride;
+    ws.n_walks = paths->n_walks;
+    ws.id_base = 0;
+    // The walk stream and the trainer stream are ordered by synchronising here.
+    dg::DeviceGuard guard(s->device);
+    DG_CUDA(cudaStreamSynchronize(paths->g->stream));
+    return train_walks(s, ws, alpha, info);
+}
+
+extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t n_walks, const uint32_t *vertices,
+                                  float alpha, dg_train_info *info) {
+    DG_CHECK(s && offsets && (vertices || offsets[n_walks] == 0), DG_ERR_ARG, "dg_sgns_train_host: NULL argument");
+    const uint64_t total = offsets[n_walks];
+    for (uint64_t i = 0; i < total; i++)
+        DG_CHECK(vertices[i] < s->v_num, DG_ERR_ARG, "vertex %u >= v_num %u", vertices[i], s->v_num);
+    dg::DeviceGuard guard(s->device);
+    dg::DevArray<uint64_t> d_off;
+    dg::DevArray<uint32_t> d_verts;
+    DG_CUDA(d_off.alloc((size_t)n_walks + 1));
+    DG_CUDA(d_verts.alloc(total ? total : 1));
+    DG_CUDA(cudaMemcpyAsync(d_off.p, offsets, ((size_t)n_walks + 1) * 8, cudaMemcpyHostToDevice, s->stream));
+    if (total) DG_CUDA(cudaMemcpyAsync(d_verts.p, vertices, total * 4, cudaMemcpyHostToDevice, s->stream));
+    dgs::WalkSet ws{};
+    ws.verts = d_verts.p;
+    ws.offsets = d_off.p;
+    ws.n_walks = n_walks;
+    ws.id_base = 0;
+    return train_walks(s, ws, alpha, info);
+}
+
+extern "C" int dg_sgns_copy_embedding(const dg_sgns *s, float *rows, uint32_t *vocab_ids, uint32_t *n_rows) {
+    DG_CHECK(s, DG_ERR_ARG, "dg_sgns_copy_embedding: NULL trainer");
+    if (n_rows) *n_rows = s->vocab_size;
+    if (vocab_ids) memcpy(vocab_ids, s->vocab_ids.data(), s->vocab_ids.size() * 4);
+    if (!rows) return DG_OK;
+    dg::DeviceGuard guard(s->device);
+    return dgs::copy_rows(s, true, rows);
+}
+
+extern "C" int dg_sgns_copy_output(const dg_sgns *s, float *rows) {
+    DG_CHECK(s && rows, DG_ERR_ARG, "dg_sgns_copy_output: NULL argument");
+    dg::DeviceGuard guard(s->device);
+    return dgs::copy_rows(s, false, rows);
+}
+
+extern "C" int dg_sgns_copy_tables(const dg_sgns *s, int32_t *table, uint32_t *keep_thr, int32_t *v2w,
+                                   float *exp_table) {
+    DG_CHECK(s, DG_ERR_ARG, "dg_sgns_copy_tables: NULL trainer");
+    dg::DeviceGuard guard(s->device);
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    if (table) DG_CUDA(cudaMemcpy(table, s->table.p, s->table.bytes(), cudaMemcpyDeviceToHost));
+    if (keep_thr) DG_CUDA(cudaMemcpy(keep_thr, s->keep_thr.p, s->keep_thr.bytes(), cudaMemcpyDeviceToHost));
+    if (v2w) DG_CUDA(cudaMemcpy(v2w, s->v2w.p, s->v2w.bytes(), cudaMemcpyDeviceToHost));
+    if (exp_table) DG_CUDA(cudaMemcpy(exp_table, s->exp_table.p, s->exp_table.bytes(), cudaMemcpyDeviceToHost));
+    return DG_OK;
+}
+
+extern "C" int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info) {
+    DG_CHECK(s && info, DG_ERR_ARG, "dg_sgns_get_info: NULL argument");
+    info->vocab_size = s->vocab_size;
+    info->master_rows = s->n_master;
+    info->train_words = s->train_words;
+    info->table_size = s->p.table_size;
+    info->device_bytes = s->v2w.bytes() + s->keep_thr.bytes() + s->table.bytes() + s->exp_table.bytes() +
+                         s->syn0.bytes() + s->syn1.bytes() + s->in_bf.bytes() + s->out_bf.bytes() +
+                         s->in_master.bytes() + s->out_master.bytes() + s->scratch.bytes();
+    return DG_OK;
+}
+
+extern "C" int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *output_rows) {
+    DG_CHECK(s, DG_ERR_ARG, "dg_sgns_set_rows: NULL trainer");
+    dg::DeviceGuard guard(s->device);
+    const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
+    for (int k = 0; k < 2; k++) {
+        const float *src = k == 0 ? input_rows : output_rows;
+        if (!src) continue;
+        if (s->p.mode == DG_SGNS_PLAIN) {
+            DG_CUDA(cudaMemcpyAsync(k == 0 ? s->syn0.p : s->syn1.p, src, n * 4, cudaMemcpyHostToDevice, s->stream));
+        } else {
+            dg::DevArray<float> tmp;
+            DG_CUDA(tmp.alloc(n));
+            DG_CUDA(cudaMemcpyAsync(tmp.p, src, n * 4, cudaMemcpyHostToDevice, s->stream));
+            dgs::rows_from_f32<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(
+                tmp.p, n, (uint64_t)s->n_master * s->p.size, k == 0 ? s->in_bf.p : s->out_bf.p,
+                k == 0 ? s->in_master.p : s->out_master.p);
+            DG_CUDA(cudaGetLastError());
+            DG_CUDA(cudaStreamSynchronize(s->stream));
+        }
+    }
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    return DG_OK;
+}
+
+// Embedding text (word2vec.cu:1353-1362): "%lld %lld\n", then per row the word
+// (the vertex id in decimal), a space, size x "%lf ", "\n".  Rows are formatted
+// by host threads in blocks and written in order.
+extern "C" int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path) {
+    DG_CHECK(s && file_path, DG_ERR_ARG, "dg_sgns_write_embedding: NULL argument");
+    const uint32_t rows = s->vocab_size;
+    const int d = s->p.size;
+    std::vector<float> emb((size_t)rows * d);
+    dg::DeviceGuard guard(s->device);
+    int rc = dgs::copy_rows(s, true, emb.data());
+    if (rc) return rc;
+    FILE *f = fopen(file_path, "wb");
+    DG_CHECK(f != nullptr, DG_ERR_IO, "cannot open %s for writing", file_path);
+    fprintf(f, "%lld %lld\n", (long long)rows, (long long)d);
+    const uint32_t block = 4096;
+    unsigned n_threads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    bool ok = true;
+    for (uint32_t base = 0; base < rows && ok; base += block * n_threads) {
+        std::vector<std::string> parts(n_threads);
+        std::vector<std::thread> th;
+        for (unsigned t = 0; t < n_threads; t++) {
+            th.emplace_back([&, t] {
+                const uint32_t lo = base + t * block, hi = std::min<uint32_t>(rows, lo + block);
+                std::string &out = parts[t];
+                char buf[64];
+                for (uint32_t r = lo; r < hi; r++) {
+                    int k = snprintf(buf, sizeof(buf), "%u ", s->vocab_ids[r]);
+                    out.append(buf, k);
+                    for (int j = 0; j < d; j++) {
+                        k = snprintf(buf, sizeof(buf), "%lf ", (double)emb[(size_t)r * d + j]);
+                        out.append(buf, k);
+                    }
+                    out.push_back('\n');
+                }
+            });
+        }
+        for (auto &x : th) x.join();
+        for (auto &p : parts)
+            if (!p.empty() && fwrite(p.data(), 1, p.size(), f) != p.size()) ok = false;
+    }
+    const int cl = fclose(f);
+    DG_CHECK(ok && cl == 0, DG_ERR_IO, "short write to %s", file_path);
+    return DG_OK;
+}

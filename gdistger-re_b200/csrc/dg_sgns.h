@@ -1,0 +1,94 @@
+// Internal declarations of the SGNS trainer (not part of the C ABI).
+#pragma once
+
+#include "dg_internal.h"
+#include "dg_philox.cuh"
+
+#include <cuda_bf16.h>
+
+#include <string>
+#include <vector>
+
+namespace dgs {
+
+constexpr int kExpTableSize = 1000;               // word2vec.cu:29
+constexpr int kMaxExp = 6;                        // word2vec.cu:30
+constexpr uint64_t kDefaultTableSize = 100000000; // word2vec.cu:66
+constexpr uint32_t kMaxSentence = 1024;           // tokens of one walk used for training
+constexpr int kPlainThreads = 256;
+constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
+
+// Philox counter word 3 of each random choice (counter words 0-2: index, walk, pass).
+constexpr uint32_t kSubTag = 0x53554253u;  // subsampling of token i
+constexpr uint32_t kWinTag = 0x57494E44u;  // window shrink of centre p
+constexpr uint32_t kNegTag = 0x4E454730u;  // negatives of pair (p, slot), + j / 4
+
+// Walks to train on: slot layout (verts + w * stride, lens[w]) or compact
+// (verts + offsets[w] .. offsets[w + 1]).
+struct WalkSet {
+    const uint32_t *verts = nullptr;
+    const uint32_t *lens = nullptr;
+    const uint64_t *offsets = nullptr;
+    const uint32_t *ids = nullptr;  // walk id for the random counters (default: index + id_base)
+    uint32_t stride = 0;
+    uint32_t n_walks = 0;
+    uint32_t id_base = 0;
+    __device__ __forceinline__ void range(uint32_t w, uint64_t &begin, uint32_t &len) const {
+        if (offsets) {
+            begin = offsets[w];
+            len = (uint32_t)(offsets[w + 1] - begin);
+        } else {
+            begin = (uint64_t)w * stride;
+            len = lens[w];
+        }
+    }
+};
+
+struct SgnsArgs {
+    const int32_t *v2w;
+    const uint32_t *keep_thr;
+    const int32_t *table;
+    const float *exp_table;
+    float *syn0, *syn1;                 // plain form, FP32 rows
+    __nv_bfloat16 *in_bf, *out_bf;      // minibatch form, BF16 rows
+    float *in_master, *out_master;      // minibatch form, FP32 rows of the hottest words
+    uint32_t n_master;
+    uint32_t *queue;
+    unsigned long long *stats;          // words, trained, pairs
+    uint64_t table_size;
+    uint64_t train_words;
+    uint32_t vocab_size;
+    int window, negative, d;
+    float alpha;
+    uint32_t pass, seed_lo, seed_hi;
+    int deterministic;
+};
+
+int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+
+}  // namespace dgs
+
+struct dg_sgns {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    dg_sgns_params p{};
+    uint32_t v_num = 0;
+    uint32_t vocab_size = 0;
+    uint32_t n_master = 0;
+    uint64_t train_words = 0;
+    uint32_t pass = 0;
+    std::vector<uint32_t> vocab_ids, vocab_cn;
+    std::vector<int32_t> h_v2w;
+    dg::DevArray<int32_t> v2w;
+    dg::DevArray<uint32_t> keep_thr;
+    dg::DevArray<int32_t> table;
+    dg::DevArray<float> exp_table;
+    dg::DevArray<float> syn0, syn1;
+    dg::DevArray<__nv_bfloat16> in_bf, out_bf;
+    dg::DevArray<float> in_master, out_master;
+    dg::DevArray<float> scratch;       // minibatch form: per-worker negative pools and cache snapshots
+    dg::DevArray<uint32_t> queue;
+    dg::DevArray<unsigned long long> stats;
+    ~dg_sgns();
+};

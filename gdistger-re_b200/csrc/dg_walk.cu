@@ -6,6 +6,7 @@
 // with explicit round-to-nearest intrinsics so that every operation is one IEEE
 // rounding in the order of include/walk.hpp:284-354.
 #include "dg_internal.h"
+#include "dg_philox.cuh"
 
 #include <cmath>
 #include <cstring>
@@ -18,21 +19,8 @@ constexpr int kSmemSteps = 24;           // footprints cached per thread in shar
 constexpr uint32_t kWalkTag = 0x57414C4Bu; // Philox counter word 3 for walk draws ("WALK")
 constexpr uint32_t kDefaultStride = 64;
 
-// Philox4x32-10 (Salmon et al., SC'11).  Seeded replay: one block per transition
-// attempt, counter = (attempt, walker, round, tag), key = seed.
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; r++) {
-        if (r) {
-            k0 += 0x9E3779B9u;
-            k1 += 0xBB67AE85u;
-        }
-        const uint32_t lo0 = 0xD2511F53u * c.x, hi0 = __umulhi(0xD2511F53u, c.x);
-        const uint32_t lo1 = 0xCD9E8D57u * c.z, hi1 = __umulhi(0xCD9E8D57u, c.z);
-        c = make_uint4(hi1 ^ c.y ^ k0, lo1, hi0 ^ c.w ^ k1, lo0);
-    }
-    return c;
-}
+// Seeded replay: one Philox block per transition attempt, counter = (attempt,
+// walker, round, tag), key = seed.
 
 struct WalkArgs {
     const uint64_t *__restrict__ offsets;

@@ -44,12 +44,17 @@ class SgnsParams(C.Structure):
     _fields_ = [("size", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("batch_size", C.c_int),
                 ("sample", C.c_float), ("alpha", C.c_float), ("iter", C.c_int), ("min_count", C.c_int),
                 ("mode", C.c_int), ("deterministic", C.c_int), ("seed", C.c_uint64),
-                ("table_size", C.c_uint64)]
+                ("table_size", C.c_uint64), ("master_rows", C.c_uint32)]
 
 
 class TrainInfo(C.Structure):
     _fields_ = [("words", C.c_uint64), ("trained", C.c_uint64), ("pairs", C.c_uint64),
                 ("train_ms", C.c_double)]
+
+
+class SgnsInfo(C.Structure):
+    _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("train_words", C.c_uint64),
+                ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
 _P = C.c_void_p
@@ -75,6 +80,8 @@ _SIGS = {
     "dg_sgns_copy_output": ([_P, _P], C.c_int),
     "dg_sgns_set_rows": ([_P, _P, _P], C.c_int),
     "dg_sgns_write_embedding": ([_P, C.c_char_p], C.c_int),
+    "dg_sgns_copy_tables": ([_P, _P, _P, _P, _P], C.c_int),
+    "dg_sgns_get_info": ([_P, C.POINTER(SgnsInfo)], C.c_int),
 }
 
 _lib = None

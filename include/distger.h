@@ -146,6 +146,7 @@ typedef struct {
     int deterministic; /* 1: one warp trains everything in order (tests, replay) */
     uint64_t seed;
     uint64_t table_size; /* unigram table slots; 0 = 1e8 (word2vec.cu:66) */
+    uint32_t master_rows; /* minibatch mode: hottest rows kept in FP32; 0 = 65536, >= vocabulary = all */
 } dg_sgns_params;
 
 /* Vocabulary from per-vertex counts (word2vec.cu:791-809 uses in+out degree,
@@ -176,6 +177,22 @@ DG_API int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t n_wa
  * gives the vertex of each row.  Either pointer may be NULL. */
 DG_API int dg_sgns_copy_embedding(const dg_sgns *s, float *rows, uint32_t *vocab_ids, uint32_t *n_rows);
 DG_API int dg_sgns_copy_output(const dg_sgns *s, float *rows);
+
+/* The trainer's lookup tables (each may be NULL): unigram table[table_size],
+ * subsampling keep thresholds[vocabulary] (a token is kept iff 16 random bits
+ * are below it), vertex -> vocabulary row map[v_num] (-1 = not in vocabulary),
+ * expTable[1001]. */
+DG_API int dg_sgns_copy_tables(const dg_sgns *s, int32_t *table, uint32_t *keep_thr, int32_t *v2w,
+                               float *exp_table);
+
+typedef struct {
+    uint32_t vocab_size;
+    uint32_t master_rows;  /* rows held in FP32 (minibatch form) */
+    uint64_t train_words;  /* sum of the vocabulary counts */
+    uint64_t table_size;
+    uint64_t device_bytes;
+} dg_sgns_info;
+DG_API int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info);
 DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *output_rows);
 
 /* Embedding text: "%lld %lld\n" header then per row "%u " + size x "%lf " + "\n"

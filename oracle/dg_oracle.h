@@ -114,6 +114,49 @@ void dgo_stream_free(void *s);
 uint32_t dgo_stream_cand(void *s, uint32_t degree);
 uint32_t dgo_stream_acc(void *s);
 
+/* ------------------------------------------------------------------ SGNS -- */
+
+/* Philox counter word 3 of the trainer's random choices. */
+#define DGO_SUB_TAG 0x53554253u /* subsampling: counter (token index, walk, pass, tag) */
+#define DGO_WIN_TAG 0x57494E44u /* window shrink: (centre position, walk, pass, tag) */
+#define DGO_NEG_TAG 0x4E454730u /* negatives: (pair index, walk, pass, tag + j/4), word j%4 */
+
+typedef struct {
+    int d, window, negative;
+    double alpha;
+    uint64_t seed;
+    uint32_t pass;
+    uint32_t vocab_size;
+    uint64_t table_size;
+    const int32_t *table;
+    const uint32_t *keep_thr;
+    const int32_t *v2w;
+    const float *exp_table;
+} dgo_sgns_cfg;
+
+typedef struct {
+    uint64_t words, trained, pairs;
+} dgo_sgns_stats;
+
+int dgo_vocab_build(const uint32_t *counts, uint32_t v_num, int min_count, uint32_t *vocab_ids, uint32_t *vocab_cn,
+                    int32_t *v2w, uint32_t *vocab_size, uint64_t *train_words);
+void dgo_unigram_table(const uint32_t *cn, uint32_t vocab_size, uint64_t table_size, int32_t *table);
+void dgo_keep_thresholds(const uint32_t *cn, uint32_t vocab_size, float sample, uint64_t train_words, int dsgl_form,
+                         uint32_t *thr);
+void dgo_init_rows(uint32_t vocab_size, int d, float *syn0);
+void dgo_exp_table(float *t);
+int dgo_sgns_plain(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                   const uint32_t *walk_ids, double *syn0, double *syn1, dgo_sgns_stats *st);
+/* dsgl.hpp Train_SGNS_MPI semantics, one worker over all walks (walk id = index). */
+int dgo_sgns_minibatch(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                       double *syn0, double *syn1, dgo_sgns_stats *st);
+/* The same two rules in FP32 in the device kernels' exact operation order
+ * (dg_oracle_sgns32.c): bit-exact against the deterministic device mode. */
+int dgo_sgns_plain_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                       float *syn0, float *syn1, dgo_sgns_stats *st);
+int dgo_sgns_minibatch_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                           float *syn0, float *syn1, dgo_sgns_stats *st);
+
 #ifdef __cplusplus
 }
 #endif

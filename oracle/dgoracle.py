@@ -84,6 +84,20 @@ def lib():
         L.dgo_philox.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.dgo_walk_ids.argtypes = [C.POINTER(_Csr), C.POINTER(_WalkParams), C.c_uint32, C.c_void_p, C.c_uint32,
                                    C.POINTER(_Paths), C.POINTER(WalkStats)]
+        L.dgo_vocab_build.argtypes = [C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                      C.c_void_p, C.c_void_p]
+        L.dgo_unigram_table.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_void_p]
+        L.dgo_keep_thresholds.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_uint64, C.c_int, C.c_void_p]
+        L.dgo_init_rows.argtypes = [C.c_uint32, C.c_int, C.c_void_p]
+        L.dgo_exp_table.argtypes = [C.c_void_p]
+        L.dgo_sgns_plain.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                     C.c_void_p, C.c_void_p]
+        L.dgo_sgns_minibatch.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+        L.dgo_sgns_plain_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p]
+        L.dgo_sgns_minibatch_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -208,6 +222,88 @@ def load_golden(path: str):
         rounds.append((z[f"offsets_{r}"], z[f"verts_{r}"]))
         r += 1
     return rounds, z["abs_delta_h"], z["meta"]
+
+
+class _SgnsCfg(C.Structure):
+    _fields_ = [("d", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("alpha", C.c_double),
+                ("seed", C.c_uint64), ("pass_", C.c_uint32), ("vocab_size", C.c_uint32),
+                ("table_size", C.c_uint64), ("table", C.c_void_p), ("keep_thr", C.c_void_p),
+                ("v2w", C.c_void_p), ("exp_table", C.c_void_p)]
+
+
+class SgnsStats(C.Structure):
+    _fields_ = [("words", C.c_uint64), ("trained", C.c_uint64), ("pairs", C.c_uint64)]
+
+
+class Sgns:
+    """FP64 SGNS checker: vocabulary, tables and both update rules."""
+
+    def __init__(self, counts: np.ndarray, size: int = 128, window: int = 10, negative: int = 5,
+                 sample: float = 1e-3, alpha: float = 0.025, min_count: int = 0, seed: int = 0,
+                 table_size: int = 100_000_000, dsgl_form: bool = False):
+        L = lib()
+        counts = np.ascontiguousarray(counts, dtype=np.uint32)
+        v_num = counts.size
+        self.vocab_ids = np.zeros(v_num, np.uint32)
+        self.vocab_cn = np.zeros(v_num, np.uint32)
+        self.v2w = np.zeros(v_num, np.int32)
+        vs = C.c_uint32()
+        tw = C.c_uint64()
+        rc = L.dgo_vocab_build(counts.ctypes.data, v_num, min_count, self.vocab_ids.ctypes.data,
+                               self.vocab_cn.ctypes.data, self.v2w.ctypes.data, C.byref(vs), C.byref(tw))
+        if rc:
+            raise RuntimeError("vocab build failed")
+        self.vocab_size = vs.value
+        self.train_words = tw.value
+        self.vocab_ids = self.vocab_ids[:self.vocab_size]
+        self.vocab_cn = self.vocab_cn[:self.vocab_size]
+        self.table = np.zeros(table_size, np.int32)
+        L.dgo_unigram_table(self.vocab_cn.ctypes.data, self.vocab_size, table_size, self.table.ctypes.data)
+        self.keep_thr = np.zeros(self.vocab_size, np.uint32)
+        L.dgo_keep_thresholds(self.vocab_cn.ctypes.data, self.vocab_size, C.c_float(sample), tw.value,
+                              int(dsgl_form), self.keep_thr.ctypes.data)
+        self.exp_table = np.zeros(1001, np.float32)
+        L.dgo_exp_table(self.exp_table.ctypes.data)
+        init = np.zeros(self.vocab_size * size, np.float32)
+        L.dgo_init_rows(self.vocab_size, size, init.ctypes.data)
+        self.syn0 = init.astype(np.float64).reshape(self.vocab_size, size)
+        self.syn1 = np.zeros((self.vocab_size, size), np.float64)
+        # FP32 rows updated in the device kernels' operation order.
+        self.syn0_f32 = init.reshape(self.vocab_size, size).copy()
+        self.syn1_f32 = np.zeros((self.vocab_size, size), np.float32)
+        self.stats_f32 = SgnsStats()
+        self.size, self.window, self.negative, self.alpha, self.seed = size, window, negative, alpha, seed
+        self.pass_ = 0
+        self.stats = SgnsStats()
+
+    def _cfg(self, alpha):
+        return _SgnsCfg(d=self.size, window=self.window, negative=self.negative,
+                        alpha=self.alpha if alpha is None else alpha, seed=self.seed, pass_=self.pass_,
+                        vocab_size=self.vocab_size, table_size=self.table.size, table=self.table.ctypes.data,
+                        keep_thr=self.keep_thr.ctypes.data, v2w=self.v2w.ctypes.data,
+                        exp_table=self.exp_table.ctypes.data)
+
+    def train(self, offsets: np.ndarray, verts: np.ndarray, minibatch: bool = False, alpha=None):
+        offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+        verts = np.ascontiguousarray(verts, dtype=np.uint32)
+        cfg = self._cfg(alpha)
+        n = offsets.size - 1
+        L = lib()
+        if minibatch:
+            rc = L.dgo_sgns_minibatch(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n,
+                                      self.syn0.ctypes.data, self.syn1.ctypes.data, C.byref(self.stats))
+            rc |= L.dgo_sgns_minibatch_f32(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n,
+                                           self.syn0_f32.ctypes.data, self.syn1_f32.ctypes.data,
+                                           C.byref(self.stats_f32))
+        else:
+            rc = L.dgo_sgns_plain(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n, None,
+                                  self.syn0.ctypes.data, self.syn1.ctypes.data, C.byref(self.stats))
+            rc |= L.dgo_sgns_plain_f32(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n,
+                                       self.syn0_f32.ctypes.data, self.syn1_f32.ctypes.data,
+                                       C.byref(self.stats_f32))
+        if rc:
+            raise RuntimeError("sgns oracle failed")
+        self.pass_ += 1
 
 
 def entropy_table(max_sn: int) -> np.ndarray:

@@ -1,0 +1,389 @@
+#!/usr/bin/env python
+"""Benchmark of DistGER's embedding hot path on B200: walk rounds streamed into SGNS.
+
+Workload (N=1): the YouTube-shaped graph -- Chung-Lu power law, exponent 2.1,
+1,138,499 vertices, ~2.99M undirected edges (3.25M records after the generator's
+isolated-vertex fix), max expected degree 28,000, edge data uniform(0,1] FP32 --
+with the reference walk defaults (--min_L 20, w = V walkers per round) and SGNS
+d=128, window 10, negative 5, sample 1e-3, alpha 0.01, iter 1, FP32 Hogwild (the
+plain form).  One step = one walk round of V walks + SGNS over those walks.
+Synthetic data: none of the paper's graphs ship with the reference.
+
+value  = walk-steps embedded per second: footprints walked and trained per
+         second of device time (CUDA events from the walk launch to the end of
+         training), summed over ranks / max over ranks of the time;
+e2e    = the same through the C ABI with host buffers: walks copied to pinned
+         host memory (dg_paths_copy) and trained from there (dg_sgns_train_host),
+         copies inside the timed region;
+--impl reference: the reference's own walk engine + dsgl trainer compiled from
+         its sources (oracle/_ref/ref_embed) on the host cores, same metric.
+
+Multi-GPU: the path does not shard (one process, one GPU per the task); N GPUs
+run N independent replicas (weak scaling), each rank on LOCAL_RANK's device.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import ctypes as C
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gdistger-re_b200"))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+METRIC = "walk-steps/s + SGNS words/s, end-to-end embed time; BF16 vs FP32 plain at equal AUC"
+UNIT = "walk-steps/s"
+WORKLOAD = {"graph": "youtube-shaped chung-lu", "vertices": 1_138_499, "undirected_edges": 2_990_443,
+            "exponent": 2.1, "max_degree": 28_000, "min_L": 20, "walkers_per_round": 1_138_499,
+            "size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.01, "iter": 1,
+            "min_count": 0}
+# Algorithmic bytes per unit (roofline section).
+BYTES_PER_PAIR_PLAIN = lambda d, n: 2 * (2 + n) * d * 4          # noqa: E731  context + 1+n targets, read+write
+BYTES_PER_DRAW, BYTES_PER_FOOTPRINT = 28, 4
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.TemporaryFile(mode="w+")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.out.seek(0)
+        rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return rank, world, local, pg
+
+
+def reduce_max(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def reduce_sum(pg, x: float) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64)
+    pg.all_reduce(t, op=pg.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def make_graph_edges():
+    from distger import graphgen
+    return graphgen.chung_lu(**graphgen.CONFIGS["c2_youtube"])
+
+
+def ref_baseline(edges_path: str, v_num: int, rounds: int, sgns_words: int, timeout: int = 900):
+    """Runs the reference walk engine + dsgl (oracle/_ref/ref_embed) on the host cores.
+    Returns per-round walk seconds, footprints, and dsgl words / seconds."""
+    import dgoracle
+    exe = os.path.join(dgoracle.HERE, "_ref", "ref_embed")
+    if not os.path.exists(exe):
+        return None
+    cores = os.cpu_count() or 1
+    walk_threads = max(1, cores - 1)   # GraphEngine's worker_num = hw threads - 1 (graph.hpp:307)
+    with tempfile.TemporaryDirectory() as tmp:
+        cmd = [exe, "-g", edges_path, "-v", str(v_num), "-w", str(v_num), "--min_L", "20", "--min_R", "1",
+               "--make-undirected", "-t", str(walk_threads), "-o", os.path.join(tmp, "w"),
+               "--walk-rounds", str(rounds), "--sgns-words", str(sgns_words), "-size", "128", "-window", "10",
+               "-negative", "5", "-sample", "1e-3", "-alpha", "0.01", "-iter", "1", "-min-count", "0",
+               "-threads", str(cores), "-debug", "0", "-eoutput", os.path.join(tmp, "emb.txt")]
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout).stdout
+    rounds_info = []
+    sgns = None
+    train_s = None
+    for line in out.splitlines():
+        if line.startswith("ref_round"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            rounds_info.append((float(kv["walk_s"]), int(kv["footprints"]), int(kv["walks"])))
+        if "Train SGNS MPI TIME" in line:
+            train_s = float(line.split(":]")[1].strip())
+        if line.startswith("ref_embed"):
+            kv = dict(x.split("=") for x in line.split()[1:])
+            sgns = int(kv["sgns_words"])
+    return {"rounds": rounds_info, "sgns_words": sgns, "sgns_train_s": train_s, "cores": cores,
+            "walk_threads": walk_threads}
+
+
+def pipeline_rate(walk_steps_per_s: float, words_per_s: float) -> float:
+    """Footprints walked and trained per second when both stages run back to back."""
+    return 1.0 / (1.0 / walk_steps_per_s + 1.0 / words_per_s)
+
+
+def run_reference(args, rank, world, pg):
+    if rank != 0:
+        return
+    edges = make_graph_edges()
+    from distger import graphgen
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "g.bin")
+        graphgen.write_edges(path, edges)
+        res = ref_baseline(path, 1_138_499, args.warmup + args.steps, args.ref_sgns_words)
+    if res is None or len(res["rounds"]) < args.warmup + args.steps or not res["sgns_train_s"]:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_embed missing or failed "
+                          "(reference walk engine + dsgl built by make -C oracle ref)"}))
+        return
+    timed = res["rounds"][args.warmup:]
+    walk_s = sum(r[0] for r in timed)
+    steps = sum(r[1] - r[2] for r in timed)
+    walk_rate = steps / walk_s
+    word_rate = res["sgns_words"] / res["sgns_train_s"]
+    value = pipeline_rate(walk_rate, word_rate)
+    ms = 1e3 * sum(r[1] for r in timed) / value / len(timed)
+    sample = (f"C2 graph, {len(res['rounds'])} walk rounds of V walkers (walk.hpp internal_random_walk, "
+              f"{res['walk_threads']} threads), dsgl on the first {res['sgns_words']} corpus tokens "
+              f"({res['cores']} threads)")
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": dict(WORKLOAD, workload="c2_youtube_plain"),
+            "walk_steps_per_s": walk_rate, "sgns_words_per_s": word_rate,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "reference",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def load_traffic():
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def run_ours(args, rank, world, local, pg):
+    import numpy as np
+    import torch
+    import distger
+    from distger import _lib
+    from distger._lib import check, lib
+    from distger.sgns import SGNS
+
+    torch.cuda.set_device(local)
+    L = lib()
+    edges = make_graph_edges()
+    v_num = 1_138_499
+    graph = distger.Graph(v_num, edges=edges, make_undirected=True, device=local)
+    csr = graph.csr()
+    counts = csr["out_deg"] + csr["in_deg"]              # word2vec vocabulary from degrees (huge_walk.cpp:43-46)
+    mode = args.mode
+    sgns = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
+                min_count=0, mode=mode, seed=1 + rank, device=local)
+    wp = _lib.WalkParams(min_len=20, init_round=10, walker_num=v_num, max_len=64, seed=2024 + rank)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
+
+    def step(r):
+        info = _lib.PipelineInfo()
+        check(L.dg_pipeline_round(graph.handle, sgns.handle, C.byref(wp), r, v_num, C.c_float(0.0),
+                                  C.byref(info), None))
+        return info
+
+    for i in range(args.warmup):
+        step(2 + i)
+    clocks = Clocks(local) if rank == 0 else None
+    if clocks:
+        clocks.start()
+    barrier(pg)
+    torch.cuda.synchronize()
+    l0 = L.dg_launch_count()
+    tot_ms = walk_ms = train_ms = 0.0
+    fp = steps_ = draws = words = pairs = 0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        info = step(2 + args.warmup + k)
+        tot_ms += info.total_ms
+        walk_ms += info.walk.walk_ms
+        train_ms += info.train.train_ms
+        fp += info.walk.footprints
+        steps_ += info.walk.steps
+        draws += info.walk.draws
+        words += info.train.words
+        pairs += info.train.pairs
+    torch.cuda.synchronize()
+    barrier(pg)
+    launches = L.dg_launch_count() - l0
+    clk = clocks.stop() if clocks else None
+
+    # e2e: the reference-facing calls with host buffers (pinned), copies timed.
+    n_walks = v_num
+    cap = n_walks * 64
+    h_off = torch.empty(n_walks + 1, dtype=torch.int64, pin_memory=True)
+    h_verts = torch.empty(cap, dtype=torch.int32, pin_memory=True)
+    e2e_s = 0.0
+    e2e_fp = 0
+    h2d = d2h = 0
+    for k in range(args.steps + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ph = C.c_void_p()
+        check(L.dg_walk_run_round(graph.handle, C.byref(wp), 100 + k, n_walks, C.byref(ph)))
+        ri = _lib.RoundInfo()
+        check(L.dg_paths_get_info(ph, C.byref(ri)))
+        check(L.dg_paths_copy(ph, h_off.data_ptr(), h_verts.data_ptr()))
+        L.dg_paths_free(ph)
+        ti = _lib.TrainInfo()
+        check(L.dg_sgns_train_host(sgns.handle, h_off.data_ptr(), n_walks, h_verts.data_ptr(), C.c_float(0.0),
+                                   C.byref(ti)))
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        if k == 0:
+            continue   # warm-up of the host path (allocations)
+        e2e_s += dt
+        e2e_fp += ri.footprints
+        d2h += (n_walks + 1) * 8 + ri.footprints * 4 + 32
+        h2d += (n_walks + 1) * 8 + ri.footprints * 4
+    t_dev = reduce_max(pg, tot_ms / 1e3)
+    all_fp = reduce_sum(pg, fp)
+    value = all_fp / t_dev
+    e2e_t = reduce_max(pg, e2e_s)
+    e2e_value = reduce_sum(pg, e2e_fp) / e2e_t
+
+    # Roofline of the dominant kernel.
+    hbm, peak_kind = peaks()
+    traffic = load_traffic()
+    if train_ms >= walk_ms:
+        kern = "sgns_plain" if mode == "plain" else "sgns_minibatch"
+        alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else None
+        kms = train_ms
+        per = traffic.get(kern, {}).get("dram_bytes_per_pair")
+        tr = per * pairs / args.steps if per else None
+    else:
+        kern = "walk"
+        alg = draws * BYTES_PER_DRAW + fp * BYTES_PER_FOOTPRINT
+        kms = walk_ms
+        per = traffic.get("walk", {}).get("dram_bytes_per_draw")
+        tr = per * draws / args.steps if per else None
+    roof = None
+    if alg is not None:
+        achieved = alg / (kms / 1e3) / 1e9
+        roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": tr,
+                "algorithmic_bytes_per_launch": alg / args.steps}
+
+    line = None
+    if rank == 0:
+        cpu = None
+        if world == 1 and not args.no_cpu_baseline:
+            from distger import graphgen
+            with tempfile.TemporaryDirectory() as tmp:
+                path = os.path.join(tmp, "g.bin")
+                graphgen.write_edges(path, edges)
+                res = ref_baseline(path, v_num, 1, args.ref_sgns_words)
+            if res and res["rounds"] and res["sgns_train_s"]:
+                w_s, f_, n_ = res["rounds"][0]
+                cv = pipeline_rate((f_ - n_) / w_s, res["sgns_words"] / res["sgns_train_s"])
+                cpu = {"value": cv, "unit": UNIT, "cores": res["cores"], "kind": "reference",
+                       "sample": f"one walk round of V walkers on the same graph ({res['walk_threads']} threads) + "
+                                 f"dsgl on {res['sgns_words']} tokens ({res['cores']} threads)",
+                       "walk_steps_per_s": (f_ - n_) / w_s,
+                       "sgns_words_per_s": res["sgns_words"] / res["sgns_train_s"]}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == "plain" else "bf16",
+                "data": "synthetic",
+                "config": dict(WORKLOAD, workload="c2_youtube_plain" if mode == "plain" else "c2_youtube_minibatch",
+                               sgns_form=mode, l2="flushed between steps (256 MB write)",
+                               parallelism=f"replicas x{world}"),
+                "walk_steps_per_s": steps_ / (walk_ms / 1e3), "sgns_words_per_s": words / (train_ms / 1e3),
+                "walk_ms_per_step": walk_ms / args.steps, "sgns_ms_per_step": train_ms / args.steps,
+                "footprints_per_step": fp / args.steps, "pairs_per_step": pairs / args.steps,
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
+                        "d2h_bytes_per_step": d2h / args.steps},
+                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu}
+    sgns.close()
+    graph.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["plain", "minibatch"], default="plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
+    args = ap.parse_args()
+    rank, world, local, pg = dist_init()
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world, pg)
+        else:
+            line = run_ours(args, rank, world, local, pg)
+            if rank == 0 and line is not None:
+                print(json.dumps(line))
+    finally:
+        if pg is not None:
+            pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

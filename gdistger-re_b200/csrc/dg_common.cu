@@ -1,6 +1,7 @@
 // Error reporting and small device utilities shared by the distger sources.
 #include "dg_internal.h"
 
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 
@@ -27,6 +28,10 @@ int cuda_fail(cudaError_t e, const char *what) {
 }
 
 void clear_error() { g_last_error.clear(); }
+
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 int sm_count(int device) {
     int n = 0;
@@ -122,9 +127,9 @@ int exclusive_scan_u32_to_u64(const uint32_t *in, uint64_t *out, uint64_t n, cud
     uint64_t tiles = (n + SCAN_TILE - 1) / SCAN_TILE;
     DevArray<uint64_t> sums;
     DG_CUDA(sums.alloc(tiles));
-    scan_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums.p);
-    scan_tile_offsets<<<1, SCAN_THREADS, 0, s>>>(sums.p, tiles);
-    scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums.p, out);
+    scan_tile_sums<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums.p); dg::note_launch();
+    scan_tile_offsets<<<1, SCAN_THREADS, 0, s>>>(sums.p, tiles); dg::note_launch();
+    scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, s>>>(in, n, sums.p, out); dg::note_launch();
     DG_CUDA(cudaGetLastError());
     DG_CUDA(cudaStreamSynchronize(s));
     return DG_OK;
@@ -135,3 +140,5 @@ int exclusive_scan_u32_to_u64(const uint32_t *in, uint64_t *out, uint64_t n, cud
 extern "C" const char *dg_last_error(void) { return dg::g_last_error.c_str(); }
 
 extern "C" const char *dg_version(void) { return "distger 0.1 sm_100a"; }
+
+extern "C" uint64_t dg_launch_count(void) { return dg::g_launches.load(std::memory_order_relaxed); }

@@ -147,7 +147,7 @@ int build_graph(const HostEdge *edges, uint64_t n_edges, uint32_t v_num, int und
         t.start(g->stream);
         int blocks = dg::sm_count(device) * 8;
         threshold_kernel<<<blocks, 256, 0, g->stream>>>(g->offsets.p, d_nbr.p, d_data.p, g->out_deg.p, v_num,
-                                                        g->entries.p);
+                                                        g->entries.p); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         t.stop(g->stream);
         DG_CUDA(cudaStreamSynchronize(g->stream));
@@ -250,7 +250,7 @@ extern "C" int dg_graph_copy_csr(const dg_graph *g, uint64_t *offsets, uint32_t 
         dg::DevArray<uint32_t> a, b;
         if (neighbours) DG_CUDA(a.alloc(g->m));
         if (thresholds) DG_CUDA(b.alloc(g->m));
-        split_entries<<<dg::sm_count(g->device) * 4, 256, 0, g->stream>>>(g->entries.p, g->m, a.p, b.p);
+        split_entries<<<dg::sm_count(g->device) * 4, 256, 0, g->stream>>>(g->entries.p, g->m, a.p, b.p); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaStreamSynchronize(g->stream));
         if (neighbours) DG_CUDA(cudaMemcpy(neighbours, a.p, g->m * 4, cudaMemcpyDeviceToHost));

@@ -88,6 +88,9 @@ struct EventTimer {
 
 int sm_count(int device);
 
+// Counts kernel launches issued by this library (reported by dg_launch_count).
+void note_launch();
+
 // Exclusive prefix sum of n 32-bit counts into 64-bit offsets (out has n + 1
 // entries; out[n] = total).  Scratch is allocated internally.
 int exclusive_scan_u32_to_u64(const uint32_t *in, uint64_t *out, uint64_t n, cudaStream_t s);

@@ -342,7 +342,7 @@ int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 #define DG_PLAIN_CASE(V)                                                                       \
     case V:                                                                                    \
         if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_kernel<V>); \
-        sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                        \
+        sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws); dg::note_launch();     \
         break;
         DG_PLAIN_CASE(1)
         DG_PLAIN_CASE(2)
@@ -382,7 +382,7 @@ int copy_rows(const dg_sgns *s, bool input, float *host) {
     DG_CUDA(tmp.alloc(n));
     rows_to_f32<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(input ? s->in_bf.p : s->out_bf.p,
                                                                      input ? s->in_master.p : s->out_master.p, n,
-                                                                     (uint64_t)s->n_master * s->p.size, tmp.p);
+                                                                     (uint64_t)s->n_master * s->p.size, tmp.p); dg::note_launch();
     DG_CUDA(cudaGetLastError());
     DG_CUDA(cudaMemcpyAsync(host, tmp.p, n * 4, cudaMemcpyDeviceToHost, s->stream));
     DG_CUDA(cudaStreamSynchronize(s->stream));
@@ -450,7 +450,7 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     if (p->mode == DG_SGNS_PLAIN) {
         DG_CUDA(s->syn0.alloc(n));
         DG_CUDA(s->syn1.alloc(n));
-        init_rows_f32<<<blocks, 256, 0, s->stream>>>(s->syn0.p, n, p->size);
+        init_rows_f32<<<blocks, 256, 0, s->stream>>>(s->syn0.p, n, p->size); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaMemsetAsync(s->syn1.p, 0, n * 4, s->stream));
     } else {
@@ -460,7 +460,7 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
         DG_CUDA(s->out_bf.alloc(n));
         DG_CUDA(s->in_master.alloc(nm));
         DG_CUDA(s->out_master.alloc(nm));
-        init_rows_bf16<<<blocks, 256, 0, s->stream>>>(s->in_bf.p, s->in_master.p, n, nm, p->size);
+        init_rows_bf16<<<blocks, 256, 0, s->stream>>>(s->in_bf.p, s->in_master.p, n, nm, p->size); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaMemsetAsync(s->out_bf.p, 0, n * 2, s->stream));
         DG_CUDA(cudaMemsetAsync(s->out_master.p, 0, nm * 4, s->stream));
@@ -535,6 +535,43 @@ extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alph
     dg::DeviceGuard guard(s->device);
     DG_CUDA(cudaStreamSynchronize(paths->g->stream));
     return train_walks(s, ws, alpha, info);
+}
+
+extern "C" int dg_pipeline_round(dg_graph *g, dg_sgns *s, const dg_walk_params *p, uint32_t round, uint32_t n_walkers,
+                                 float alpha, dg_pipeline_info *info, dg_paths **keep) {
+    DG_CHECK(g && s && p, DG_ERR_ARG, "dg_pipeline_round: NULL argument");
+    DG_CHECK(g->device == s->device, DG_ERR_ARG, "graph and trainer live on different devices");
+    if (keep) *keep = nullptr;
+    dg::DeviceGuard guard(g->device);
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    DG_CUDA(cudaEventCreate(&t0));
+    DG_CUDA(cudaEventCreate(&t1));
+    struct Ev {
+        cudaEvent_t &a, &b;
+        ~Ev() { cudaEventDestroy(a); cudaEventDestroy(b); }
+    } ev{t0, t1};
+    DG_CUDA(cudaEventRecord(t0, g->stream));
+    dg_paths *paths = nullptr;
+    int rc = dg_walk_run_round(g, p, round, n_walkers, &paths);
+    if (rc) return rc;
+    dg_train_info tinfo{};
+    rc = dg_sgns_train_paths(s, paths, alpha, &tinfo);
+    if (rc) {
+        dg_paths_free(paths);
+        return rc;
+    }
+    DG_CUDA(cudaEventRecord(t1, s->stream));
+    DG_CUDA(cudaEventSynchronize(t1));
+    float ms = 0.f;
+    DG_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+    if (info) {
+        info->walk = paths->info;
+        info->train = tinfo;
+        info->total_ms = ms;
+    }
+    if (keep) *keep = paths;
+    else dg_paths_free(paths);
+    return DG_OK;
 }
 
 extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t n_walks, const uint32_t *vertices,
@@ -612,7 +649,7 @@ extern "C" int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float
             DG_CUDA(cudaMemcpyAsync(tmp.p, src, n * 4, cudaMemcpyHostToDevice, s->stream));
             dgs::rows_from_f32<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(
                 tmp.p, n, (uint64_t)s->n_master * s->p.size, k == 0 ? s->in_bf.p : s->out_bf.p,
-                k == 0 ? s->in_master.p : s->out_master.p);
+                k == 0 ? s->in_master.p : s->out_master.p); dg::note_launch();
             DG_CUDA(cudaGetLastError());
             DG_CUDA(cudaStreamSynchronize(s->stream));
         }

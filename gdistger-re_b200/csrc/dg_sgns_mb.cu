@@ -450,6 +450,7 @@ int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     case 128: sgns_mb_kernel<128><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
     case 256: sgns_mb_kernel<256><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
     }
+    dg::note_launch();
     DG_CUDA(cudaGetLastError());
     return DG_OK;
 }

@@ -229,7 +229,7 @@ int relative_entropy(dg_graph *g, uint64_t words_sum, double *h) {
     dg::DevArray<double> partial;
     DG_CUDA(partial.alloc(blocks));
     entropy_partials<<<blocks, kEntropyThreads, 0, g->stream>>>(g->out_deg.p, g->freq.p, g->v_num, (double)g->m,
-                                                                  (double)words_sum, partial.p);
+                                                                  (double)words_sum, partial.p); dg::note_launch();
     DG_CUDA(cudaGetLastError());
     std::vector<double> host(blocks);
     DG_CUDA(cudaMemcpyAsync(host.data(), partial.p, blocks * sizeof(double), cudaMemcpyDeviceToHost, g->stream));
@@ -292,7 +292,7 @@ int run_round(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_w
 
     dg::EventTimer t;
     t.start(g->stream);
-    walk_kernel<<<(unsigned)blocks, kWalkThreads, 0, g->stream>>>(a);
+    walk_kernel<<<(unsigned)blocks, kWalkThreads, 0, g->stream>>>(a); dg::note_launch();
     DG_CUDA(cudaGetLastError());
     t.stop(g->stream);
     unsigned long long h_stats[4];
@@ -368,7 +368,7 @@ extern "C" int dg_paths_copy(const dg_paths *ps, uint64_t *offsets, uint32_t *ve
         dg::DevArray<uint32_t> flat;
         DG_CUDA(flat.alloc(ps->info.footprints));
         compact_walks<<<dg::sm_count(ps->device) * 8, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride,
-                                                                     at.p, flat.p);
+                                                                     at.p, flat.p); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaStreamSynchronize(s));
         DG_CUDA(cudaMemcpy(vertices, flat.p, ps->info.footprints * 4, cudaMemcpyDeviceToHost));
@@ -385,7 +385,7 @@ extern "C" int dg_paths_write_text(const dg_paths *ps, const char *file_path) {
     dg::DevArray<uint64_t> at;
     DG_CUDA(nbytes.alloc(ps->n_walks ? ps->n_walks : 1));
     DG_CUDA(at.alloc((size_t)ps->n_walks + 1));
-    text_lengths<<<blocks, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride, nbytes.p);
+    text_lengths<<<blocks, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride, nbytes.p); dg::note_launch();
     DG_CUDA(cudaGetLastError());
     int rc = dg::exclusive_scan_u32_to_u64(nbytes.p, at.p, ps->n_walks, s);
     if (rc) return rc;
@@ -395,7 +395,7 @@ extern "C" int dg_paths_write_text(const dg_paths *ps, const char *file_path) {
     if (total) {
         dg::DevArray<char> text;
         DG_CUDA(text.alloc(total));
-        text_write<<<blocks, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride, at.p, text.p);
+        text_write<<<blocks, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride, at.p, text.p); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaStreamSynchronize(s));
         DG_CUDA(cudaMemcpy(host.data(), text.p, total, cudaMemcpyDeviceToHost));

@@ -52,6 +52,10 @@ class TrainInfo(C.Structure):
                 ("train_ms", C.c_double)]
 
 
+class PipelineInfo(C.Structure):
+    _fields_ = [("walk", RoundInfo), ("train", TrainInfo), ("total_ms", C.c_double)]
+
+
 class SgnsInfo(C.Structure):
     _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("train_words", C.c_uint64),
                 ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
@@ -82,6 +86,9 @@ _SIGS = {
     "dg_sgns_write_embedding": ([_P, C.c_char_p], C.c_int),
     "dg_sgns_copy_tables": ([_P, _P, _P, _P, _P], C.c_int),
     "dg_sgns_get_info": ([_P, C.POINTER(SgnsInfo)], C.c_int),
+    "dg_pipeline_round": ([_P, _P, C.POINTER(WalkParams), C.c_uint32, C.c_uint32, C.c_float,
+                           C.POINTER(PipelineInfo), C.POINTER(_P)], C.c_int),
+    "dg_launch_count": ([], C.c_uint64),
 }
 
 _lib = None

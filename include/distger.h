@@ -199,6 +199,24 @@ DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *ou
  * (word2vec.cu:1353-1362). */
 DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
 
+/* --------------------------------------------------------------- pipeline */
+
+typedef struct {
+    dg_round_info walk;
+    dg_train_info train;
+    double total_ms;   /* device time from the walk launch to the end of training (CUDA events) */
+} dg_pipeline_info;
+
+/* One round streamed straight into the trainer: dg_walk_run_round followed by
+ * dg_sgns_train_paths on the device-resident walks, ordered on the device (no
+ * host copy of the walks).  The walks are freed unless keep is non-NULL, in
+ * which case *keep receives them. */
+DG_API int dg_pipeline_round(dg_graph *g, dg_sgns *s, const dg_walk_params *p, uint32_t round, uint32_t n_walkers,
+                             float alpha, dg_pipeline_info *info, dg_paths **keep);
+
+/* Number of kernels this library has launched in the process so far. */
+DG_API uint64_t dg_launch_count(void);
+
 #ifdef __cplusplus
 }
 #endif

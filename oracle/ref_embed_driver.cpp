@@ -87,7 +87,19 @@ int main(int argc, char **argv) {
         fflush(stdout);
         _exit(0);
     };
+    double last_t = 0.0, last_other = 0.0;
     walk_conf.set_output_consumer([&](PathSet *paths) {
+        // Per-round walk time: wall time since the previous round minus the
+        // engine's own assemble + dump time of this round.
+        size_t fp = 0, walks = 0;
+        for (int s = 0; s < paths->seg_num; s++)
+            for (walker_id_t w = 0; w < paths->path_num[s]; w++) { fp += paths->path_length[s][w]; walks++; }
+        const double now = walk_timer.duration();
+        printf("\nref_round r=%d walk_s=%.6f walks=%zu footprints=%zu\n", rounds_done + 1,
+               (now - last_t) - (engine.other_time - last_other), walks, fp);
+        fflush(stdout);
+        last_t = now;
+        last_other = engine.other_time;
         delete paths;
         if (++rounds_done >= walk_rounds) finish();
     });

@@ -25,6 +25,7 @@
 #include "dg_sgns.h"
 
 #include <algorithm>
+#include <mutex>
 
 namespace dgs {
 
@@ -456,3 +457,150 @@ int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 }
 
 }  // namespace dgs
+
+// ---------------------------------------------------------------------------
+// Allocation-free entry point: the minibatch trainer with its per-worker
+// scratch (negative pools and cache snapshots) in a fixed device array that is
+// part of this library, so that a call performs no device or host allocation.
+// It serves callers that must not allocate: code running inside a CUDA graph
+// capture, a memory pool owned by a framework that forbids foreign cudaMalloc,
+// or a real-time loop that cannot pay an allocator's latency or failure modes.
+// ---------------------------------------------------------------------------
+namespace dgs {
+namespace {
+
+// Scratch shared by every call on a device (held by each GPU that loads the library).
+constexpr size_t kNoAllocScratchBytes = 16u << 20;
+constexpr int kNoAllocMaxDevices = 64;
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchBytes / sizeof(float)];
+static __device__ __align__(256) unsigned long long g_noalloc_stats[4];
+
+// Device address of the scratch array, looked up once per device (the host-side
+// name of a __device__ array is not a device address).
+struct NoAllocSetup {
+    std::mutex mu;
+    float *scratch[kNoAllocMaxDevices] = {};
+    unsigned long long *stats[kNoAllocMaxDevices] = {};
+};
+NoAllocSetup &noalloc_setup() {
+    static NoAllocSetup s;
+    return s;
+}
+
+int noalloc_pointers(int device, float **scratch, unsigned long long **stats) {
+    DG_CHECK(device >= 0 && device < kNoAllocMaxDevices, DG_ERR_ARG, "device %d beyond the %d supported", device,
+             kNoAllocMaxDevices);
+    NoAllocSetup &s = noalloc_setup();
+    std::lock_guard<std::mutex> lock(s.mu);
+    if (!s.scratch[device]) {
+        void *p = nullptr, *q = nullptr;
+        DG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        DG_CUDA(cudaGetSymbolAddress(&q, g_noalloc_stats));
+        s.scratch[device] = static_cast<float *>(p);
+        s.stats[device] = static_cast<unsigned long long *>(q);
+    }
+    *scratch = s.scratch[device];
+    *stats = s.stats[device];
+    return DG_OK;
+}
+
+}  // namespace
+}  // namespace dgs
+
+extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, void *stream, dg_train_info *info) {
+    using namespace dgs;
+    DG_CHECK(x, DG_ERR_ARG, "dg_sgns_minibatch_train_noalloc: NULL arguments");
+    DG_CHECK(x->verts && x->offsets && x->v2w && x->keep_thr && x->table && x->exp_table, DG_ERR_ARG,
+             "dg_sgns_minibatch_train_noalloc: walk or table pointer is NULL");
+    DG_CHECK(x->in_bf16 && x->out_bf16 && (x->n_master == 0 || (x->in_master && x->out_master)), DG_ERR_ARG,
+             "dg_sgns_minibatch_train_noalloc: row pointer is NULL");
+    const int d = x->size;
+    DG_CHECK(d == 32 || d == 64 || d == 128 || d == 256, DG_ERR_ARG, "size %d not supported (32, 64, 128, 256)", d);
+    DG_CHECK(x->window >= 1 && x->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", x->window);
+    DG_CHECK(x->negative >= 0 && x->negative <= 22, DG_ERR_ARG, "negative %d out of range [0, 22]", x->negative);
+    DG_CHECK(x->vocab_size > 0 && x->table_size > 0 && x->table_size < (1ull << 32), DG_ERR_ARG,
+             "empty vocabulary or unigram table");
+    int device = 0;
+    DG_CUDA(cudaGetDevice(&device));
+    float *scratch = nullptr;
+    unsigned long long *stats = nullptr;
+    int rc = noalloc_pointers(device, &scratch, &stats);
+    if (rc) return rc;
+
+    MbArgs m{};
+    m.pool_cap = (uint32_t)kMbMaxSent * (uint32_t)std::max(x->negative, 1);
+    m.max_out = x->negative + 2;
+    m.max_in = 4 * x->window;
+    m.scratch_stride = (uint64_t)m.pool_cap * d * 2 + 2ull * kMbMaxSent * d;
+    m.scratch = scratch;
+    const uint64_t per_worker = m.scratch_stride * sizeof(float);
+    const uint64_t max_workers = kNoAllocScratchBytes / per_worker;
+    DG_CHECK(max_workers >= 1, DG_ERR_ARG,
+             "size %d with negative %d needs %llu bytes of scratch per worker, more than the %zu-byte static area",
+             d, x->negative, (unsigned long long)per_worker, kNoAllocScratchBytes);
+    const size_t smem = mb_smem_bytes(d, m.max_out, m.max_in, m.pool_cap);
+    int per_sm = 1;
+    auto setup = [&](auto kern) -> int {
+        DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMbThreads, smem));
+        return DG_OK;
+    };
+    switch (d) {
+    case 32: rc = setup(sgns_mb_kernel<32>); break;
+    case 64: rc = setup(sgns_mb_kernel<64>); break;
+    case 128: rc = setup(sgns_mb_kernel<128>); break;
+    default: rc = setup(sgns_mb_kernel<256>); break;
+    }
+    if (rc) return rc;
+    DG_CHECK(per_sm >= 1, DG_ERR_ARG, "minibatch kernel does not fit (%zu bytes of shared memory)", smem);
+    uint64_t workers = x->deterministic ? 1 : (uint64_t)dg::sm_count(device) * per_sm;
+    workers = std::min<uint64_t>(workers, max_workers);
+    if (workers > x->n_walks / 2 + 1) workers = std::max<uint64_t>(1, x->n_walks / 2);
+
+    SgnsArgs a{};
+    a.v2w = x->v2w;
+    a.keep_thr = x->keep_thr;
+    a.table = x->table;
+    a.exp_table = x->exp_table;
+    a.in_bf = reinterpret_cast<__nv_bfloat16 *>(x->in_bf16);
+    a.out_bf = reinterpret_cast<__nv_bfloat16 *>(x->out_bf16);
+    a.in_master = x->in_master;
+    a.out_master = x->out_master;
+    a.n_master = x->n_master;
+    a.stats = stats;
+    a.table_size = x->table_size;
+    a.vocab_size = x->vocab_size;
+    a.window = x->window;
+    a.negative = x->negative;
+    a.d = d;
+    a.alpha = x->alpha;
+    a.pass = x->pass;
+    a.seed_lo = (uint32_t)x->seed;
+    a.seed_hi = (uint32_t)(x->seed >> 32);
+    a.deterministic = x->deterministic;
+    WalkSet ws{};
+    ws.verts = x->verts;
+    ws.offsets = x->offsets;
+    ws.n_walks = x->n_walks;
+
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    DG_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s));  // counters start at zero every call
+    switch (d) {
+    case 32: sgns_mb_kernel<32><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
+    case 64: sgns_mb_kernel<64><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
+    case 128: sgns_mb_kernel<128><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
+    default: sgns_mb_kernel<256><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
+    }
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    if (info) {
+        unsigned long long st[4];
+        DG_CUDA(cudaMemcpyAsync(st, stats, sizeof(st), cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        info->words = st[0];
+        info->trained = st[1];
+        info->pairs = st[2];
+        info->train_ms = 0.0;
+    }
+    return DG_OK;
+}

@@ -56,6 +56,17 @@ class PipelineInfo(C.Structure):
     _fields_ = [("walk", RoundInfo), ("train", TrainInfo), ("total_ms", C.c_double)]
 
 
+class MinibatchArgs(C.Structure):
+    """dg_sgns_minibatch_args: device pointers for the allocation-free trainer."""
+    _fields_ = [("verts", C.c_void_p), ("offsets", C.c_void_p), ("n_walks", C.c_uint32),
+                ("v2w", C.c_void_p), ("keep_thr", C.c_void_p), ("table", C.c_void_p),
+                ("table_size", C.c_uint64), ("exp_table", C.c_void_p), ("vocab_size", C.c_uint32),
+                ("in_bf16", C.c_void_p), ("out_bf16", C.c_void_p), ("in_master", C.c_void_p),
+                ("out_master", C.c_void_p), ("n_master", C.c_uint32), ("size", C.c_int), ("window", C.c_int),
+                ("negative", C.c_int), ("alpha", C.c_float), ("seed", C.c_uint64), ("pass_", C.c_uint32),
+                ("deterministic", C.c_int)]
+
+
 class SgnsInfo(C.Structure):
     _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("train_words", C.c_uint64),
                 ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
@@ -89,6 +100,7 @@ _SIGS = {
     "dg_pipeline_round": ([_P, _P, C.POINTER(WalkParams), C.c_uint32, C.c_uint32, C.c_float,
                            C.POINTER(PipelineInfo), C.POINTER(_P)], C.c_int),
     "dg_launch_count": ([], C.c_uint64),
+    "dg_sgns_minibatch_train_noalloc": ([C.POINTER(MinibatchArgs), _P, C.POINTER(TrainInfo)], C.c_int),
 }
 
 _lib = None

@@ -217,6 +217,49 @@ DG_API int dg_pipeline_round(dg_graph *g, dg_sgns *s, const dg_walk_params *p, u
 /* Number of kernels this library has launched in the process so far. */
 DG_API uint64_t dg_launch_count(void);
 
+/* ------------------------------------------------ allocation-free trainer */
+
+/* Arguments of dg_sgns_minibatch_train_noalloc: every pointer is device memory
+ * owned by the caller.  Tables and rows have the layouts dg_sgns_copy_tables
+ * and dg_sgns_copy_embedding describe; rows are updated in place. */
+typedef struct {
+    const uint32_t *verts;     /* walk vertices */
+    const uint64_t *offsets;   /* n_walks + 1 offsets into verts */
+    uint32_t n_walks;
+    const int32_t *v2w;        /* vertex -> vocabulary row, -1 = skipped */
+    const uint32_t *keep_thr;  /* subsampling keep thresholds per vocabulary row */
+    const int32_t *table;      /* unigram table */
+    uint64_t table_size;
+    const float *exp_table;    /* 1001 sigmoid entries */
+    uint32_t vocab_size;
+    uint16_t *in_bf16;         /* vocab_size x size input rows, BF16 bits */
+    uint16_t *out_bf16;        /* vocab_size x size output rows, BF16 bits */
+    float *in_master;          /* n_master x size FP32 input rows (rows 0..n_master-1) */
+    float *out_master;         /* n_master x size FP32 output rows */
+    uint32_t n_master;
+    int size;                  /* 32, 64, 128 or 256 */
+    int window, negative;      /* negative <= 22 */
+    float alpha;
+    uint64_t seed;
+    uint32_t pass;             /* pass counter: one value per call, as dg_sgns_train_* count them */
+    int deterministic;         /* 1: one worker, walks in order */
+} dg_sgns_minibatch_args;
+
+/* No counterpart in the reference.  The minibatch trainer (DG_SGNS_MINIBATCH)
+ * with no allocation at all, for callers that cannot call cudaMalloc: code that
+ * runs while a CUDA graph is being captured, code whose device memory belongs to
+ * a framework's pool, or a latency-bound loop that cannot wait on an allocator.
+ * Its per-worker scratch (negative pools, cache snapshots) lives in a 16 MiB
+ * device array that is part of this library and is held by every GPU that loads
+ * it until the process exits; sizes whose per-worker scratch exceeds it are
+ * DG_ERR_ARG, and the number of parallel workers is capped by it.  The first
+ * call on a device looks up the array's device address, so make that first call
+ * before any stream capture.  Every call shares the array: calls whose work
+ * overlaps on the GPU (other streams, other threads) race and must not be issued.
+ * stream is a cudaStream_t (NULL = legacy default stream).  With info non-NULL
+ * the call waits for the stream and reports the counters (train_ms = 0). */
+DG_API int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *args, void *stream, dg_train_info *info);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,95 @@
+"""The allocation-free minibatch trainer against the handle-based one.
+
+dg_sgns_minibatch_train_noalloc exists for callers that cannot allocate device
+memory (graph capture, framework-owned memory pools, latency-bound loops): the
+caller owns every buffer and the trainer's scratch lives in a fixed array inside
+the library.  Here the caller's buffers come from torch, are filled with the
+tables and initial rows of a handle-based trainer with the same parameters, and
+two calls in a row must leave the rows equal to what the handle's two
+dg_sgns_train_host calls produce (deterministic mode: identical, so the
+tolerance of the other SGNS tests, exact FP32 agreement, applies).
+This file is collected last on purpose.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+pytestmark = pytest.mark.gpu
+
+
+def _walks_and_counts():
+    import dgoracle
+    from distger import graphgen
+    rounds, _, _ = dgoracle.load_golden(os.path.join(GOLDEN, "tiny200_ref_walks.npz"))
+    edges = graphgen.read_edges(os.path.join(GOLDEN, "tiny200.bin"))
+    csr = dgoracle.Csr(edges, 200, undirected=True)
+    return rounds[0], (csr.out_deg + csr.in_deg).astype(np.uint32)
+
+
+def _rows_from_device(bf16_t, master_t, n_master):
+    bits = bf16_t.cpu().numpy().astype(np.uint16).astype(np.uint32) << 16
+    rows = bits.view(np.float32).copy()
+    rows[:n_master] = master_t.cpu().numpy()[:n_master]
+    return rows
+
+
+def test_noalloc_minibatch_matches_handle_two_calls(distger_lib):
+    import torch
+    from distger import _lib
+    from distger._lib import check, lib
+    from distger.sgns import SGNS
+
+    (offs, verts), counts = _walks_and_counts()
+    size, n_master = 64, 16
+    ref = SGNS(200, counts, size=size, window=5, negative=5, sample=1e-3, alpha=0.025, min_count=0,
+               mode="minibatch", deterministic=True, seed=11, table_size=1_000_000, master_rows=n_master)
+    t = ref.tables()
+    rows0, _ = ref.embedding()
+    vs = ref.vocab_size
+    dev = torch.device("cuda:0")
+    u16 = (rows0.view(np.uint32) >> 16).astype(np.uint16)
+    in_bf = torch.from_numpy(u16.view(np.int16).copy()).to(dev)
+    out_bf = torch.zeros((vs, size), dtype=torch.int16, device=dev)
+    in_m = torch.from_numpy(rows0[:n_master].copy()).to(dev)
+    out_m = torch.zeros((n_master, size), dtype=torch.float32, device=dev)
+    v2w = torch.from_numpy(t["v2w"]).to(dev)
+    keep = torch.from_numpy(t["keep_thr"].view(np.int32)).to(dev)
+    table = torch.from_numpy(t["table"]).to(dev)
+    expt = torch.from_numpy(t["exp_table"]).to(dev)
+    torch.cuda.synchronize()
+
+    for call in range(2):
+        lo, hi = 50 * call, 50 * call + 50
+        o = (offs[lo:hi + 1] - offs[lo]).astype(np.uint64)
+        v = verts[int(offs[lo]):int(offs[hi])].astype(np.uint32)
+        want = ref.train_host(o, v)
+        d_off = torch.from_numpy(o.view(np.int64)).to(dev)
+        d_v = torch.from_numpy(v.view(np.int32)).to(dev)
+        torch.cuda.synchronize()
+        a = _lib.MinibatchArgs(verts=d_v.data_ptr(), offsets=d_off.data_ptr(), n_walks=hi - lo,
+                               v2w=v2w.data_ptr(), keep_thr=keep.data_ptr(), table=table.data_ptr(),
+                               table_size=table.numel(), exp_table=expt.data_ptr(), vocab_size=vs,
+                               in_bf16=in_bf.data_ptr(), out_bf16=out_bf.data_ptr(), in_master=in_m.data_ptr(),
+                               out_master=out_m.data_ptr(), n_master=n_master, size=size, window=5, negative=5,
+                               alpha=0.025, seed=11, pass_=call, deterministic=1)
+        got = _lib.TrainInfo()
+        check(lib().dg_sgns_minibatch_train_noalloc(C.byref(a), None, C.byref(got)))
+        assert (got.words, got.trained, got.pairs) == (want.words, want.trained, want.pairs)
+        exp_in, _ = ref.embedding()
+        exp_out = ref.output_rows()
+        np.testing.assert_array_equal(_rows_from_device(in_bf, in_m, n_master), exp_in, err_msg=f"call {call}")
+        np.testing.assert_array_equal(_rows_from_device(out_bf, out_m, n_master), exp_out, err_msg=f"call {call}")
+
+
+def test_noalloc_rejects_unsupported_size(distger_lib):
+    from distger import DistgerError, _lib
+    from distger._lib import check, lib
+    a = _lib.MinibatchArgs(verts=1, offsets=1, n_walks=1, v2w=1, keep_thr=1, table=1, table_size=1, exp_table=1,
+                           vocab_size=1, in_bf16=1, out_bf16=1, in_master=1, out_master=1, n_master=1, size=512,
+                           window=5, negative=5, alpha=0.025, seed=1, pass_=0, deterministic=1)
+    with pytest.raises(DistgerError) as e:
+        check(lib().dg_sgns_minibatch_train_noalloc(C.byref(a), None, None))
+    assert e.value.code == -1 and "size 512" in str(e.value)

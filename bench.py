@@ -362,8 +362,40 @@ def run_ours(args, rank, world, local, pg):
     return line
 
 
+def run_profile_case(args, local):
+    """A small case of one kernel for ncu: the YouTube-shaped graph and trainer
+    (rows larger than L2), one walk round of --profile-walks walkers, then one
+    SGNS launch over those walks.  Prints a one-line summary."""
+    import distger
+    from distger.sgns import SGNS
+    edges = make_graph_edges()
+    v_num = 1_138_499
+    graph = distger.Graph(v_num, edges=edges, make_undirected=True, device=local)
+    csr = graph.csr()
+    counts = csr["out_deg"] + csr["in_deg"]
+    eng = distger.WalkEngine(device=local, seed=7)
+    eng.graph = graph
+    eng.set_init_round(10)
+    p1 = eng.run_round(v_num, 2, n_walkers=args.profile_walks)
+    p2 = eng.run_round(v_num, 3, n_walkers=args.profile_walks)
+    out = {"case": args.profile, "walks": args.profile_walks, "walk_ms": p2.info.walk_ms,
+           "draws": p2.info.draws, "footprints": p2.info.footprints}
+    if args.profile in ("sgns", "minibatch"):
+        s = SGNS(v_num, counts, size=128, window=10, negative=5, sample=1e-3, alpha=0.01, iter=1, min_count=0,
+                 mode="plain" if args.profile == "sgns" else "minibatch", seed=1, device=local)
+        info = s.train_paths(p2)
+        out.update({"train_ms": info.train_ms, "pairs": info.pairs, "words": info.words})
+        s.close()
+    p1.close()
+    p2.close()
+    print(json.dumps(out))
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--profile", choices=["walk", "sgns", "minibatch"], default=None,
+                    help="run one small launch of a kernel for ncu and exit")
+    ap.add_argument("--profile-walks", type=int, default=50_000)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
@@ -372,6 +404,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
     args = ap.parse_args()
+    if args.profile:
+        run_profile_case(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return
     rank, world, local, pg = dist_init()
     try:
         if args.impl == "reference":

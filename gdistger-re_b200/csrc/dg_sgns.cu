@@ -230,8 +230,129 @@ __device__ __forceinline__ uint32_t warp_sentence(const WalkSet &ws, uint32_t wa
     return n;
 }
 
+// Negative target j (1-based) of pair (centre p, window slot s) of walk wid:
+// unigram table draw with word2vec's replacement of index 0 (word2vec.cu:365-368).
+__device__ __forceinline__ int32_t negative_target(const SgnsArgs &a, uint32_t p, uint32_t s, uint32_t wid, int j) {
+    const uint4 blk = philox((uint32_t)(p * (2 * a.window + 1) + s), wid, a.pass, kNegTag + (uint32_t)((j - 1) >> 2),
+                             a.seed_lo, a.seed_hi);
+    const uint32_t q = (j - 1) & 3;
+    const uint32_t r = q == 0 ? blk.x : q == 1 ? blk.y : q == 2 ? blk.z : blk.w;
+    int32_t t = a.table[r % a.table_size];
+    if (t == 0) t = (int32_t)((r >> 8) % (a.vocab_size - 1) + 1);
+    return t;
+}
+
+// Plain SGNS with the pair's targets fetched together: lane j - 1 draws negative
+// j, every lane then issues the loads of all 1 + negative target rows and the
+// context row before any of them is consumed, so a pair costs one table round
+// trip and one row round trip instead of a chain of 1 + 2 * negative.  The
+// update order is unchanged: targets are applied in order, and a negative that
+// repeats an earlier one of the same pair is re-read from the updated copy.
+// Handles negative <= kFastNeg; larger counts use sgns_plain_seq_kernel.
+constexpr int kFastNeg = 8;
+
 template <int VEC>
 __global__ void __launch_bounds__(kPlainThreads) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[kPlainThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    const int d = 32 * VEC;
+    const float alpha = a.alpha;
+    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % (uint32_t)a.window;
+            float *pos_row = a.syn1 + (size_t)word * d + lane * VEC;
+            RowVec<VEC> pos, pos0;
+            load_row<VEC>(pos_row, pos);
+            pos0 = pos;
+            for (uint32_t s = b; s < (uint32_t)(2 * a.window + 1) - b; s++) {
+                if (s == (uint32_t)a.window) continue;
+                const int64_t c = (int64_t)p - a.window + s;
+                if (c < 0 || c >= (int64_t)n) continue;
+                const int32_t last = sen[c];
+                float *l1p = a.syn0 + (size_t)last * d + lane * VEC;
+                // Lane j - 1 draws negative j; everyone learns all targets.
+                int32_t my_t = -1;
+                if ((int)lane < neg) my_t = negative_target(a, p, s, wid, (int)lane + 1);
+                int32_t t[kFastNeg];
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++) t[j] = __shfl_sync(0xffffffffu, my_t, j);
+                // Issue every row load of the pair before consuming any.
+                RowVec<VEC> l1, e, l2[kFastNeg];
+                load_row<VEC>(l1p, l1);
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++)
+                    if (j < neg && t[j] != word) load_row<VEC>(a.syn1 + (size_t)t[j] * d + lane * VEC, l2[j]);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
+                n_pairs++;
+                {   // positive target: the centre word (kept in registers for this centre)
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++) {
+                    if (j >= neg || t[j] == word) continue;
+                    const float g = sg_grad(warp_dot<VEC>(l1, l2[j]), 0, a.exp_table, alpha);
+                    RowVec<VEC> upd;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, l2[j].v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, l1.v[i]);  // rounded product, never fused
+                        l2[j].v[i] += upd.v[i];
+                    }
+                    float *l2p = a.syn1 + (size_t)t[j] * d + lane * VEC;
+                    if (a.deterministic) store_row<VEC>(l2p, l2[j]);
+                    else add_row<VEC>(l2p, upd);
+                    // A later negative of this pair on the same row sees this update.
+#pragma unroll
+                    for (int k = j + 1; k < kFastNeg; k++)
+                        if (t[k] == t[j]) l2[k] = l2[j];
+                }
+                if (a.deterministic) {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
+                    store_row<VEC>(l1p, l1);
+                } else {
+                    add_row<VEC>(l1p, e);
+                }
+            }
+            if (a.deterministic) {
+                store_row<VEC>(pos_row, pos);
+            } else {
+#pragma unroll
+                for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
+                add_row<VEC>(pos_row, pos);
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
+// One target at a time (any negative count up to 64).
+template <int VEC>
+__global__ void __launch_bounds__(kPlainThreads) sgns_plain_seq_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[kPlainThreads / 32][kMaxSentence];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
@@ -338,11 +459,18 @@ int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
         return std::max(per_sm, 1);
     };
     if (!s->p.deterministic) threads = kPlainThreads;
+    const bool fast = a.negative <= kFastNeg;
     switch (vec) {
-#define DG_PLAIN_CASE(V)                                                                       \
-    case V:                                                                                    \
-        if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_kernel<V>); \
-        sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws); dg::note_launch();     \
+#define DG_PLAIN_CASE(V)                                                                             \
+    case V:                                                                                          \
+        if (fast) {                                                                                  \
+            if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_kernel<V>);   \
+            sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                          \
+        } else {                                                                                     \
+            if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_seq_kernel<V>); \
+            sgns_plain_seq_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                      \
+        }                                                                                            \
+        dg::note_launch();                                                                           \
         break;
         DG_PLAIN_CASE(1)
         DG_PLAIN_CASE(2)

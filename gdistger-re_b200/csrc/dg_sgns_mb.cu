@@ -12,16 +12,23 @@
 //   row 0 positive against sentence-1 columns, row O-1 against sentence-2
 //   columns (dsgl.hpp:1241-1274);
 //   outputs += corr . inputs,  inputs += corr^T . outputs (dsgl.hpp:1290-1311).
-// Sentence caches live in shared memory (FP32); the negative pool lives in this
-// CTA's slice of a global scratch area (FP32).  Caches are written back as
-// deltas when a sentence ends (inputs) or after two sentences (pool), so that
-// concurrent workers do not overwrite each other.  BF16 rows are rounded
+//
+// The worker's NW warps split the columns: warp w owns the contiguous block
+// [w*32*v, (w+1)*32*v), lane l of it v columns (v = size / (32 NW)).  Everything
+// but the corr dots is column-local, so the warps only meet once per batch of
+// 32 dots: each warp reduces its partial sums with a recursive-halving transpose
+// (31 shuffles for 32 sums; lane j ends with dot j, summed in the tree of an xor
+// butterfly), the NW partials are added in warp order, and every warp derives
+// the same gradients.  Output rows of a step sit in registers.  Sentence caches
+// live in shared memory (FP32); the negative pool lives in this worker's slice of
+// a global scratch area (FP32).  Caches are written back as deltas when a
+// sentence ends (inputs) or after two sentences (pool).  BF16 rows are rounded
 // stochastically; the hottest rows (lowest vocabulary ids) are FP32 masters
 // updated with atomics.
 //
 // The contractions are O x I x d = 7 x 40 x 128 per step for the reference
-// configuration: far below one tcgen05 tile (M >= 64), so they run as
-// thread-per-dot products and thread-per-column updates on FP32 CUDA cores.
+// configuration: far below one tcgen05 tile (M >= 64) and sequential from step
+// to step, so they run on FP32 CUDA cores.
 #include "dg_sgns.h"
 
 #include <algorithm>
@@ -29,17 +36,21 @@
 
 namespace dgs {
 
-constexpr int kMbThreads = 128;
-constexpr int kMbMaxSent = 64;              // tokens per sentence (= distinct rows per cache)
-constexpr uint32_t kMbWinTag = 0x4D425749u; // "MBWI": window shrink of step s
+constexpr int kMbMaxSent = 32;               // tokens per sentence (= cache rows per sentence)
+constexpr int kMbHash = 512;                 // pool dedup table (>= 2 x pool capacity)
+constexpr uint32_t kMbWinTag = 0x4D425749u;  // "MBWI": window shrink of step s
 constexpr uint32_t kMbPoolTag = 0x4D42504Fu; // "MBPO": negative pool sample j of pool p
 
 struct MbArgs {
-    float *scratch;            // per worker: pool_cur, pool_init (pool_cap x d each), sent_init (2 x 64 x d)
+    float *scratch;            // per worker: pool_cur, pool_init (pool_cap x d each), sent_init (2 x 32 x d)
     uint64_t scratch_stride;   // floats per worker
     uint32_t pool_cap;         // kMbMaxSent * negative
-    int max_out, max_in;
+    int max_in;                // 4 * window
+    uint32_t smem;             // bytes per worker
 };
+
+// Warps per worker for a row size: each lane owns two columns (one for d = 32).
+constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
     h ^= h >> 16;
@@ -58,49 +69,127 @@ __device__ __forceinline__ __nv_bfloat16 bf16_sr(float x, uint32_t noise) {
     return __ushort_as_bfloat16((unsigned short)(u >> 16));
 }
 
+// V consecutive columns of one row, owned by one lane.
+template <int V>
+struct Cols {
+    float v[V];
+};
+
+template <int V>
+__device__ __forceinline__ void ld_cols(const float *p, Cols<V> &c) {
+    if constexpr (V % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < V; i += 4) {
+            const float4 t = *reinterpret_cast<const float4 *>(p + i);
+            c.v[i] = t.x; c.v[i + 1] = t.y; c.v[i + 2] = t.z; c.v[i + 3] = t.w;
+        }
+    } else if constexpr (V == 2) {
+        const float2 t = *reinterpret_cast<const float2 *>(p);
+        c.v[0] = t.x; c.v[1] = t.y;
+    } else {
+        c.v[0] = p[0];
+    }
+}
+
+template <int V>
+__device__ __forceinline__ void st_cols(float *p, const Cols<V> &c) {
+    if constexpr (V % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < V; i += 4)
+            *reinterpret_cast<float4 *>(p + i) = make_float4(c.v[i], c.v[i + 1], c.v[i + 2], c.v[i + 3]);
+    } else if constexpr (V == 2) {
+        *reinterpret_cast<float2 *>(p) = make_float2(c.v[0], c.v[1]);
+    } else {
+        p[0] = c.v[0];
+    }
+}
+
+// Rows of a table: BF16 storage, with FP32 masters for rows < n_master.
+template <int V>
 struct MbRows {
     __nv_bfloat16 *bf;
     float *master;
     uint32_t n_master;
     int d;
-    __device__ __forceinline__ float get(int32_t w, int k) const {
-        return (uint32_t)w < n_master ? __ldcg(master + (size_t)w * d + k) : __bfloat162float(bf[(size_t)w * d + k]);
-    }
-    // row[w][k] += delta
-    __device__ __forceinline__ void add(int32_t w, int k, float delta, uint32_t noise) const {
+    __device__ __forceinline__ void get(int32_t w, int col, Cols<V> &c) const {
         if ((uint32_t)w < n_master) {
-            atomicAdd(master + (size_t)w * d + k, delta);
+            const float *p = master + (size_t)w * d + col;
+#pragma unroll
+            for (int i = 0; i < V; i++) c.v[i] = __ldcg(p + i);
         } else {
-            __nv_bfloat16 *p = bf + (size_t)w * d + k;
-            *p = bf16_sr(__bfloat162float(*p) + delta, noise);
+            const __nv_bfloat16 *p = bf + (size_t)w * d + col;
+#pragma unroll
+            for (int i = 0; i < V; i++) c.v[i] = __bfloat162float(p[i]);
+        }
+    }
+    __device__ __forceinline__ bool is_master(int32_t w) const { return (uint32_t)w < n_master; }
+    // The current BF16 value of a non-master row (masters need no read: they are
+    // updated with atomics).
+    __device__ __forceinline__ void load_old(int32_t w, int col, Cols<V> &old) const {
+        if ((uint32_t)w >= n_master) {
+            const __nv_bfloat16 *p = bf + (size_t)w * d + col;
+#pragma unroll
+            for (int i = 0; i < V; i++) old.v[i] = __bfloat162float(p[i]);
+        }
+    }
+    // row[w][col..col+V) += delta, given the row's value `old` (unused for masters).
+    __device__ __forceinline__ void apply(int32_t w, int col, const Cols<V> &old, const Cols<V> &delta,
+                                          uint32_t salt) const {
+        if ((uint32_t)w < n_master) {
+            float *p = master + (size_t)w * d + col;
+            if constexpr (V == 2) {
+                atomicAdd(reinterpret_cast<float2 *>(p), make_float2(delta.v[0], delta.v[1]));
+            } else {
+#pragma unroll
+                for (int i = 0; i < V; i++) atomicAdd(p + i, delta.v[i]);
+            }
+        } else {
+            __nv_bfloat16 *p = bf + (size_t)w * d + col;
+#pragma unroll
+            for (int i = 0; i < V; i++)
+                p[i] = bf16_sr(old.v[i] + delta.v[i], mix32(salt + (uint32_t)i * 0x9E3779B9u));
         }
     }
 };
 
-template <int D>
-__global__ void __launch_bounds__(kMbThreads) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
-    constexpr int LD = D + 1;                        // padded row stride (bank-conflict free)
-    constexpr int CPT = D >= kMbThreads ? D / kMbThreads : 1;
-    extern __shared__ float smem[];
-    const int tid = threadIdx.x;
-    const int MO = m.max_out, MI = m.max_in;
-    float *cache = smem;                              // [2][kMbMaxSent][LD]
-    float *outs = cache + 2 * kMbMaxSent * LD;        // [MO][LD]
-    float *gm = outs + MO * LD;                       // [MO][MI]
-    int *ip = reinterpret_cast<int *>(gm + MO * MI);
-    int *sen = ip;                                    // [2][kMbMaxSent] vocabulary ids
-    int *slot = sen + 2 * kMbMaxSent;                 // [2][kMbMaxSent] token -> cache row
-    int *dist = slot + 2 * kMbMaxSent;                // [2][kMbMaxSent] cache row -> word
-    int *in_row = dist + 2 * kMbMaxSent;              // [MI] cache row (+ kMbMaxSent for sentence 2)
-    int *out_word = in_row + MI;                      // [MO]
-    int *out_meta = out_word + MO;                    // [MO]
-    int *out_slot = out_meta + MO;                    // [MO] pool slot, -1 for centres
-    int *pool_slot = out_slot + MO;                   // [pool_cap] sample -> pool slot
-    int *pool_word = pool_slot + m.pool_cap;          // [pool_cap] pool slot -> word
+__device__ __forceinline__ float mb_grad(float f, int label, const float *exp_table, float alpha) {
+    if (f > kMaxExp) return (label - 1) * alpha;
+    if (f < -kMaxExp) return label * alpha;
+    return (label - exp_table[(int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2))]) * alpha;
+}
 
-    __shared__ int s_len[2], s_pos[2], s_ndist[2], s_walk[2];
-    __shared__ int s_npool, s_nbn, s_O, s_I, s_first;
-    __shared__ unsigned long long s_words, s_trained, s_pairs;
+// Shared memory of one worker (floats first, then ints).
+constexpr uint32_t mb_smem_bytes(int d, int out, int max_in, uint32_t pool_cap) {
+    return (uint32_t)((2u * kMbMaxSent * d + (uint32_t)mb_warps(d) * max_in * out + 2u * mb_warps(d) * 32u) * 4 +
+                      (6u * kMbMaxSent + (uint32_t)max_in + 2u * pool_cap + kMbHash + 3u * out + 16u) * 4);
+}
+
+// D: row size; OUT: output slots per step (>= negative + 2, a divisor of 32).
+template <int D, int OUT>
+__global__ void __launch_bounds__(32 * mb_warps(D)) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
+    constexpr int NW = mb_warps(D);
+    constexpr int V = D / (32 * NW);
+    constexpr int IPB = 32 / OUT;                   // inputs per batch of 32 corr dots
+    constexpr int kRowBatch = 8;                    // rows whose loads are issued together
+    extern __shared__ __align__(16) float smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int col = warp * 32 * V + lane * V;
+    const int MI = m.max_in;
+    float *cache = smem;                            // [2][kMbMaxSent][D]
+    float *gm = cache + 2 * kMbMaxSent * D + warp * MI * OUT;   // this warp's copy, [MI][OUT]
+    float *xs = cache + 2 * kMbMaxSent * D + NW * MI * OUT;     // [2][NW][32] partial dots
+    int *ip = reinterpret_cast<int *>(xs + 2 * NW * 32);
+    int *sen = ip;                                  // [2][kMbMaxSent] vocabulary ids
+    int *slot = sen + 2 * kMbMaxSent;               // [2][kMbMaxSent] token -> cache row
+    int *dist = slot + 2 * kMbMaxSent;              // [2][kMbMaxSent] cache row -> word
+    int *in_row = dist + 2 * kMbMaxSent;            // [MI] cache row (+ kMbMaxSent for sentence 2)
+    int *pool_slot = in_row + MI;                   // [pool_cap] sample -> pool slot
+    int *pool_word = pool_slot + m.pool_cap;        // [pool_cap] pool slot -> word
+    int *hash = pool_word + m.pool_cap;             // [kMbHash] word -> pool slot (dedup)
+    int *out_word = hash + kMbHash;                 // [OUT]
+    int *out_meta = out_word + OUT;                 // [OUT]
+    int *out_slot = out_meta + OUT;                 // [OUT] pool slot, -1 for centres
+    int *shr = out_slot + OUT;                      // [16] scalars: 0-1 len, 2-3 ndist, 4 npool, 5 O, 6 I, 7 first
 
     const uint32_t worker = blockIdx.x;
     const uint32_t W = ws.n_walks, G = gridDim.x;
@@ -109,349 +198,490 @@ __global__ void __launch_bounds__(kMbThreads) sgns_mb_kernel(SgnsArgs a, WalkSet
     float *pool_init = pool_cur + (uint64_t)m.pool_cap * D;
     float *sent_init = pool_init + (uint64_t)m.pool_cap * D;   // [2][kMbMaxSent][D]
     const uint32_t key0 = a.seed_lo ^ mix32(a.pass * 0x9E3779B9u + 0x632BE5ABu), key1 = a.seed_hi;
-    const MbRows in_rows{a.in_bf, a.in_master, a.n_master, D};
-    const MbRows out_rows{a.out_bf, a.out_master, a.n_master, D};
+    const MbRows<V> in_rows{a.in_bf, a.in_master, a.n_master, D};
+    const MbRows<V> out_rows{a.out_bf, a.out_master, a.n_master, D};
     const float alpha = a.alpha;
     const int window = a.window, negative = a.negative;
 
-    if (tid == 0) {
-        s_len[0] = s_len[1] = 0;
-        s_words = s_trained = s_pairs = 0;
-        s_npool = 0;
-    }
-    uint32_t next_walk = w_begin;   // uniform across the CTA
+    // Worker state, identical in every thread.
+    int len[2] = {0, 0}, pos[2] = {0, 0};
+    int nbn = 1;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    uint32_t next_walk = w_begin;
     uint32_t step = 0, pool_no = 0, neg_count = 0;
     int train_sen_num = 0;
     bool change_neg = true, pool_loaded = false;
-    __syncthreads();
 
-    // Writes back cache s as a delta against the rows it was loaded from.
+    auto salt_of = [&](int32_t w, uint32_t extra) {
+        return mix32(key0 ^ mix32((uint32_t)w * 0x01000193u + (uint32_t)col) ^ (step * 0x2545F491u) ^ extra);
+    };
+    // Writes cache s back as a delta against the rows it was loaded from.
+    // Rows of one flush are distinct, so all their reads are issued before any write.
     auto flush_sentence = [&](int s) {
-        const int nd = s_ndist[s];
-        for (int r = 0; r < nd; r++) {
-            const int w = dist[s * kMbMaxSent + r];
-            for (int c = 0; c < CPT; c++) {
-                const int k = tid + c * kMbThreads;
-                if (k < D) {
-                    const float cur = cache[(s * kMbMaxSent + r) * LD + k];
-                    const float ini = sent_init[((uint64_t)s * kMbMaxSent + r) * D + k];
-                    in_rows.add(w, k, cur - ini, mix32(key0 ^ mix32(w * 0x01000193u + k) ^ (step << 1) ^ s));
+        const int nd = shr[2 + s];
+        for (int r0 = 0; r0 < nd; r0 += kRowBatch) {
+            Cols<V> cur[kRowBatch], ini[kRowBatch], old[kRowBatch];
+#pragma unroll
+            for (int u = 0; u < kRowBatch; u++)
+                if (r0 + u < nd) {
+                    ld_cols<V>(cache + (s * kMbMaxSent + r0 + u) * D + col, cur[u]);
+                    ld_cols<V>(sent_init + ((uint64_t)s * kMbMaxSent + r0 + u) * D + col, ini[u]);
+                    in_rows.load_old(dist[s * kMbMaxSent + r0 + u], col, old[u]);
                 }
-            }
+#pragma unroll
+            for (int u = 0; u < kRowBatch; u++)
+                if (r0 + u < nd) {
+#pragma unroll
+                    for (int i = 0; i < V; i++) cur[u].v[i] -= ini[u].v[i];
+                    const int w = dist[s * kMbMaxSent + r0 + u];
+                    in_rows.apply(w, col, old[u], cur[u], salt_of(w, 0x11u + s));
+                }
         }
     };
     auto flush_pool = [&]() {
-        const int np = s_npool;
-        for (int r = 0; r < np; r++) {
-            const int w = pool_word[r];
-            for (int c = 0; c < CPT; c++) {
-                const int k = tid + c * kMbThreads;
-                if (k < D) {
-                    const float d = pool_cur[(uint64_t)r * D + k] - pool_init[(uint64_t)r * D + k];
-                    out_rows.add(w, k, d, mix32(key1 ^ mix32(w * 0x01000193u + k) ^ (step << 2) ^ 0x55u));
+        const int np = shr[4];
+        for (int r0 = 0; r0 < np; r0 += kRowBatch) {
+            Cols<V> cur[kRowBatch], ini[kRowBatch], old[kRowBatch];
+#pragma unroll
+            for (int u = 0; u < kRowBatch; u++)
+                if (r0 + u < np) {
+                    ld_cols<V>(pool_cur + (uint64_t)(r0 + u) * D + col, cur[u]);
+                    ld_cols<V>(pool_init + (uint64_t)(r0 + u) * D + col, ini[u]);
+                    out_rows.load_old(pool_word[r0 + u], col, old[u]);
                 }
-            }
+#pragma unroll
+            for (int u = 0; u < kRowBatch; u++)
+                if (r0 + u < np) {
+#pragma unroll
+                    for (int i = 0; i < V; i++) cur[u].v[i] -= ini[u].v[i];
+                    out_rows.apply(pool_word[r0 + u], col, old[u], cur[u], salt_of(pool_word[r0 + u], 0x55u));
+                }
         }
     };
 
     for (;;) {
-        // ---- fill empty sentence slots (dsgl.hpp:903-1028) ----
+        // ---- fill empty sentence slots (dsgl.hpp:903-1028); warp 0 builds, all load ----
         for (int s = 0; s < 2; s++) {
-            while (true) {
-                __syncthreads();
-                if (s_len[s] != 0) break;
-                if (next_walk >= w_end) break;
+            while (len[s] == 0 && next_walk < w_end) {
                 const uint32_t walk = next_walk++;
-                if (tid < 32) {
-                    // vocabulary lookup + subsampling, compacted by ballot
-                    uint64_t begin;
-                    uint32_t len;
-                    ws.range(walk, begin, len);
-                    if (len > kMbMaxSent) len = kMbMaxSent;
+                uint64_t begin;
+                uint32_t wl;
+                ws.range(walk, begin, wl);
+                if (wl > kMbMaxSent) wl = kMbMaxSent;
+                if (warp == 0) {
                     const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
-                    uint32_t n = 0;
-                    for (uint32_t base = 0; base < len; base += 32) {
-                        const uint32_t i = base + tid;
-                        bool keep = false;
-                        int32_t w = -1;
-                        if (i < len) {
-                            w = a.v2w[ws.verts[begin + i]];
-                            if (w >= 0) {
-                                const uint32_t u = philox4x32_10(make_uint4(i, wid, a.pass, kSubTag), a.seed_lo,
-                                                                 a.seed_hi).x & 0xFFFFu;
-                                keep = u < a.keep_thr[w];
-                            }
+                    bool keep = false;
+                    int32_t w = -1;
+                    if ((uint32_t)lane < wl) {
+                        w = a.v2w[ws.verts[begin + lane]];
+                        if (w >= 0) {
+                            const uint32_t u = philox4x32_10(make_uint4((uint32_t)lane, wid, a.pass, kSubTag),
+                                                             a.seed_lo, a.seed_hi).x & 0xFFFFu;
+                            keep = u < a.keep_thr[w];
                         }
-                        const uint32_t mask = __ballot_sync(0xffffffffu, keep);
-                        if (keep) sen[s * kMbMaxSent + n + __popc(mask & ((1u << tid) - 1))] = w;
-                        n += __popc(mask);
                     }
+                    const uint32_t mask = __ballot_sync(0xffffffffu, keep);
+                    const int n = __popc(mask);
+                    if (keep) sen[s * kMbMaxSent + __popc(mask & ((1u << lane) - 1))] = w;
                     __syncwarp();
                     // distinct words in first-occurrence order (dsgl.hpp:948-956)
                     int nd = 0;
-                    for (uint32_t t = 0; t < n; t++) {
-                        const int w = sen[s * kMbMaxSent + t];
-                        const bool hit0 = tid < nd && dist[s * kMbMaxSent + tid] == w;
-                        const bool hit1 = tid + 32 < nd && dist[s * kMbMaxSent + tid + 32] == w;
-                        const uint32_t m0 = __ballot_sync(0xffffffffu, hit0), m1 = __ballot_sync(0xffffffffu, hit1);
+                    for (int t = 0; t < n; t++) {
+                        const int wt = sen[s * kMbMaxSent + t];
+                        const uint32_t hit =
+                            __ballot_sync(0xffffffffu, lane < nd && dist[s * kMbMaxSent + lane] == wt);
                         int r;
-                        if (m0) r = __ffs(m0) - 1;
-                        else if (m1) r = 32 + __ffs(m1) - 1;
-                        else {
+                        if (hit) {
+                            r = __ffs(hit) - 1;
+                        } else {
                             r = nd;
-                            if (tid == 0) dist[s * kMbMaxSent + nd] = w;
+                            if (lane == 0) dist[s * kMbMaxSent + nd] = wt;
                             nd++;
                         }
-                        if (tid == 0) slot[s * kMbMaxSent + t] = r;
+                        if (lane == 0) slot[s * kMbMaxSent + t] = r;
                         __syncwarp();
                     }
-                    if (tid == 0) {
-                        s_words += len;
-                        s_trained += n;
-                        s_len[s] = n <= 1 ? 0 : (int)n;   // dsgl.hpp:941-945
-                        s_pos[s] = 0;
-                        s_ndist[s] = nd;
-                        s_walk[s] = (int)wid;
+                    if (lane == 0) {
+                        shr[s] = n <= 1 ? 0 : n;   // dsgl.hpp:941-945
+                        shr[2 + s] = nd;
+                        shr[8 + s] = n;
                     }
                 }
                 __syncthreads();
-                if (s_len[s] != 0) {
-                    const int nd = s_ndist[s];
-                    for (int r = 0; r < nd; r++) {
-                        const int w = dist[s * kMbMaxSent + r];
-                        for (int c = 0; c < CPT; c++) {
-                            const int k = tid + c * kMbThreads;
-                            if (k < D) {
-                                const float v = in_rows.get(w, k);
-                                cache[(s * kMbMaxSent + r) * LD + k] = v;
-                                sent_init[((uint64_t)s * kMbMaxSent + r) * D + k] = v;
+                len[s] = shr[s];
+                pos[s] = 0;
+                n_words += wl;
+                n_trained += shr[8 + s];
+                if (len[s] != 0) {
+                    const int nd = shr[2 + s];
+                    for (int r0 = 0; r0 < nd; r0 += kRowBatch) {
+                        Cols<V> c[kRowBatch];
+#pragma unroll
+                        for (int u = 0; u < kRowBatch; u++)
+                            if (r0 + u < nd) in_rows.get(dist[s * kMbMaxSent + r0 + u], col, c[u]);
+#pragma unroll
+                        for (int u = 0; u < kRowBatch; u++)
+                            if (r0 + u < nd) {
+                                st_cols<V>(cache + (s * kMbMaxSent + r0 + u) * D + col, c[u]);
+                                st_cols<V>(sent_init + ((uint64_t)s * kMbMaxSent + r0 + u) * D + col, c[u]);
                             }
-                        }
                     }
                 }
+                __syncthreads();
             }
         }
-        __syncthreads();
-        if (s_len[0] == 0 || s_len[1] == 0) break;   // slice exhausted (dsgl.hpp:1029-1049)
+        if (len[0] == 0 || len[1] == 0) break;   // slice exhausted (dsgl.hpp:1029-1049)
 
         // ---- shared negative pool (dsgl.hpp:1052-1083) ----
         if (change_neg) {
-            if (tid == 0) {
-                const int nbn = max(s_len[0], s_len[1]);
+            nbn = max(len[0], len[1]);
+            if (warp == 0) {
+                const int total = nbn * negative;
+                for (int h = lane; h < kMbHash; h += 32) hash[h] = -1;
+                __syncwarp();
                 int np = 0;
-                for (int j = 0; j < nbn * negative; j++) {
-                    uint4 x = philox4x32_10(make_uint4((uint32_t)j >> 2, pool_no, worker, kMbPoolTag), key0, key1);
-                    const uint32_t q = j & 3;
-                    const uint32_t r = q == 0 ? x.x : q == 1 ? x.y : q == 2 ? x.z : x.w;
-                    int32_t smp = a.table[r % a.table_size];
-                    if (!smp) smp = a.vocab_size > 1 ? (int32_t)((r >> 8) % (a.vocab_size - 1) + 1) : 0;
-                    int at = -1;
-                    for (int t = 0; t < np; t++)
-                        if (pool_word[t] == smp) { at = t; break; }
-                    if (at < 0) { at = np; pool_word[np++] = smp; }
-                    pool_slot[j] = at;
+                for (int base = 0; base < total; base += 32) {
+                    const int j = base + lane;
+                    int32_t smp = -1;
+                    if (j < total) {
+                        const uint4 x =
+                            philox4x32_10(make_uint4((uint32_t)j >> 2, pool_no, worker, kMbPoolTag), key0, key1);
+                        const uint32_t q = j & 3;
+                        const uint32_t r = q == 0 ? x.x : q == 1 ? x.y : q == 2 ? x.z : x.w;
+                        smp = a.table[r % a.table_size];
+                        if (!smp) smp = a.vocab_size > 1 ? (int32_t)((r >> 8) % (a.vocab_size - 1) + 1) : 0;
+                    }
+                    // Pool slots in sample order (first occurrence keeps its slot).
+                    const int cnt = min(32, total - base);
+                    for (int t = 0; t < cnt; t++) {
+                        const int w = __shfl_sync(0xffffffffu, smp, t);
+                        if (lane == 0) {
+                            uint32_t h = mix32((uint32_t)w) & (kMbHash - 1);
+                            int at = -1;
+                            for (int probe = 0; probe < kMbHash; probe++) {
+                                const int e = hash[h];
+                                if (e < 0) {
+                                    at = np;
+                                    hash[h] = np;
+                                    pool_word[np++] = w;
+                                    break;
+                                }
+                                if (pool_word[e] == w) {
+                                    at = e;
+                                    break;
+                                }
+                                h = (h + 1) & (kMbHash - 1);
+                            }
+                            pool_slot[base + t] = at;
+                        }
+                    }
+                    np = __shfl_sync(0xffffffffu, np, 0);
                 }
-                s_npool = np;
-                s_nbn = nbn;
+                if (lane == 0) shr[4] = np;
             }
             __syncthreads();
-            const int np = s_npool;
-            for (int r = 0; r < np; r++) {
-                const int w = pool_word[r];
-                for (int c = 0; c < CPT; c++) {
-                    const int k = tid + c * kMbThreads;
-                    if (k < D) {
-                        const float v = out_rows.get(w, k);
-                        pool_cur[(uint64_t)r * D + k] = v;
-                        pool_init[(uint64_t)r * D + k] = v;
+            const int np = shr[4];
+            for (int r0 = 0; r0 < np; r0 += kRowBatch) {
+                Cols<V> c[kRowBatch];
+#pragma unroll
+                for (int u = 0; u < kRowBatch; u++)
+                    if (r0 + u < np) out_rows.get(pool_word[r0 + u], col, c[u]);
+#pragma unroll
+                for (int u = 0; u < kRowBatch; u++)
+                    if (r0 + u < np) {
+                        st_cols<V>(pool_cur + (uint64_t)(r0 + u) * D + col, c[u]);
+                        st_cols<V>(pool_init + (uint64_t)(r0 + u) * D + col, c[u]);
                     }
-                }
             }
             pool_no++;
             change_neg = false;
             pool_loaded = true;
         }
 
-        // ---- step bookkeeping: inputs and outputs (dsgl.hpp:1089-1160) ----
-        if (tid == 0) {
+        // ---- step bookkeeping: inputs and outputs (dsgl.hpp:1089-1160), by warp 0 ----
+        neg_count++;
+        if (warp == 0) {
             const uint32_t b = philox4x32_10(make_uint4(step, worker, 0, kMbWinTag), key0, key1).x % (uint32_t)window;
             int ni = 0;
             for (int s = 0; s < 2; s++) {
-                const int pos = s_pos[s], len = s_len[s];
-                for (int i = (int)b; i < 2 * window + 1 - (int)b; i++) {
-                    if (i == window) continue;
-                    const int c = pos - window + i;
-                    if (c < 0) continue;
-                    if (c >= len) break;
-                    in_row[ni++] = s * kMbMaxSent + slot[s * kMbMaxSent + c];
+                for (int base = (int)b; base < 2 * window + 1 - (int)b; base += 32) {
+                    const int i = base + lane;
+                    const int c = pos[s] - window + i;
+                    const bool ok = i < 2 * window + 1 - (int)b && i != window && c >= 0 && c < len[s];
+                    const uint32_t mask = __ballot_sync(0xffffffffu, ok);
+                    if (ok) in_row[ni + __popc(mask & ((1u << lane) - 1))] = s * kMbMaxSent + slot[s * kMbMaxSent + c];
+                    ni += __popc(mask);
                 }
-                if (s == 0) s_first = ni;
+                if (s == 0 && lane == 0) shr[7] = ni;
             }
-            s_I = ni;
-            neg_count++;
-            const int start = (int)(neg_count % (uint32_t)s_nbn);
-            int off = 1;
-            out_word[0] = sen[s_pos[0]];
-            out_meta[0] = 1;
-            out_slot[0] = -1;
-            for (int k = 0; k < negative; k++) {
-                const int ps = pool_slot[start * negative + k];
-                const int smp = pool_word[ps];
-                int at = -1;
-                for (int t = 0; t < off; t++)
-                    if (out_word[t] == smp) { at = t; break; }
-                if (at < 0) {
-                    out_word[off] = smp;
-                    out_meta[off] = 1;
-                    out_slot[off] = ps;
-                    off++;
-                } else {
-                    out_meta[at]++;
-                }
+            const int start = (int)(neg_count % (uint32_t)nbn);
+            const int t1 = sen[pos[0]];
+            int ps = -1, smp = -1;
+            if (lane < negative) {
+                ps = pool_slot[start * negative + lane];
+                smp = pool_word[ps];
             }
-            out_meta[0] = 1;                          // dsgl.hpp:1153-1154
-            out_word[off] = sen[kMbMaxSent + s_pos[1]];
-            out_meta[off] = 1;
-            out_slot[off] = -1;
-            s_O = off + 1;
-            s_pairs += ni;
+            const uint32_t same = __match_any_sync(0xffffffffu, smp);
+            const bool lead = lane < negative && (int)(__ffs(same) - 1) == lane && smp != t1;
+            const uint32_t leads = __ballot_sync(0xffffffffu, lead);
+            if (lead) {
+                const int o = 1 + __popc(leads & ((1u << lane) - 1));
+                out_word[o] = smp;
+                out_meta[o] = __popc(same);
+                out_slot[o] = ps;
+            }
+            if (lane == 0) {
+                const int O = 2 + __popc(leads);
+                out_word[0] = t1;
+                out_meta[0] = 1;                     // dsgl.hpp:1153-1154
+                out_slot[0] = -1;
+                out_word[O - 1] = sen[kMbMaxSent + pos[1]];
+                out_meta[O - 1] = 1;
+                out_slot[O - 1] = -1;
+                shr[5] = O;
+                shr[6] = ni;
+            }
         }
         __syncthreads();
-        const int O = s_O, I = s_I, first = s_first;
+        const int O = shr[5], I = shr[6], first = shr[7];
+        n_pairs += I;
 
-        // ---- stage output rows (target rows from the tables, negatives from the pool) ----
-        for (int o = 0; o < O; o++) {
-            const int w = out_word[o], ps = out_slot[o];
-            for (int c = 0; c < CPT; c++) {
-                const int k = tid + c * kMbThreads;
-                if (k < D) outs[o * LD + k] = ps < 0 ? out_rows.get(w, k) : pool_cur[(uint64_t)ps * D + k];
+        // ---- output rows into registers (centres from the tables, negatives from the pool) ----
+        Cols<V> x[OUT];
+#pragma unroll
+        for (int o = 0; o < OUT; o++) {
+            if (o < O) {
+                if (out_slot[o] < 0) out_rows.get(out_word[o], col, x[o]);
+                else ld_cols<V>(pool_cur + (uint64_t)out_slot[o] * D + col, x[o]);
+            } else {
+#pragma unroll
+                for (int k = 0; k < V; k++) x[o].v[k] = 0.f;
             }
         }
-        __syncthreads();
 
         // ---- corr = outputs . inputs^T, gradients (dsgl.hpp:1241-1274) ----
-        for (int q = tid; q < O * I; q += kMbThreads) {
-            const int o = q / I, i = q - o * I;
-            const float *x = outs + o * LD;
-            const float *y = cache + in_row[i] * LD;
-            float f = 0.f;
-#pragma unroll 8
-            for (int k = 0; k < D; k++) f = fmaf(x[k], y[k], f);
-            const int label = i < first ? (o == 0) : (o == O - 1);
-            float g;
-            if (f > kMaxExp) g = (label - 1) * alpha;
-            else if (f < -kMaxExp) g = label * alpha;
-            else g = (label - a.exp_table[(int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2))]) * alpha;
-            gm[o * MI + i] = g * (float)out_meta[o];
+        int parity = 0;
+        for (int i0 = 0; i0 < I; i0 += IPB, parity ^= 1) {
+            float s[32];
+#pragma unroll
+            for (int bi = 0; bi < IPB; bi++) {
+                Cols<V> y;
+                if (i0 + bi < I) ld_cols<V>(cache + in_row[i0 + bi] * D + col, y);
+                else {
+#pragma unroll
+                    for (int k = 0; k < V; k++) y.v[k] = 0.f;
+                }
+#pragma unroll
+                for (int o = 0; o < OUT; o++) {
+                    float acc = 0.f;
+#pragma unroll
+                    for (int k = 0; k < V; k++) acc = fmaf(x[o].v[k], y.v[k], acc);
+                    s[bi * OUT + o] = acc;
+                }
+            }
+            // Recursive halving: lane j ends with this warp's partial of dot j.
+#pragma unroll
+            for (int w = 16; w >= 1; w >>= 1) {
+                const bool upper = (lane & w) != 0;
+#pragma unroll
+                for (int k = 0; k < w; k++) {
+                    const float send = upper ? s[k] : s[k + w];
+                    const float keep = upper ? s[k + w] : s[k];
+                    s[k] = keep + __shfl_xor_sync(0xffffffffu, send, w);
+                }
+            }
+            float f = s[0];
+            if (NW > 1) {
+                xs[(parity * NW + warp) * 32 + lane] = f;
+                __syncthreads();
+                f = xs[parity * NW * 32 + lane];
+#pragma unroll
+                for (int w = 1; w < NW; w++) f += xs[(parity * NW + w) * 32 + lane];
+            }
+            const int bi = lane / OUT, o = lane % OUT, i = i0 + bi;
+            if (i < I && o < O) {
+                const int label = i < first ? (o == 0) : (o == O - 1);
+                gm[i * OUT + o] = mb_grad(f, label, a.exp_table, alpha) * (float)out_meta[o];
+            }
         }
-        __syncthreads();
+        __syncwarp();
 
-        // ---- outputs += corr . inputs ; inputs += corr^T . outputs (dsgl.hpp:1290-1396) ----
-        for (int c = 0; c < CPT; c++) {
-            const int k = tid + c * kMbThreads;
-            if (k >= D) continue;
-            float md[24];
+        // ---- outputs += corr . inputs (dsgl.hpp:1290-1295), from the inputs before their update ----
+        Cols<V> md[OUT];
 #pragma unroll
-            for (int o = 0; o < 24; o++) {
+        for (int o = 0; o < OUT; o++)
+#pragma unroll
+            for (int k = 0; k < V; k++) md[o].v[k] = 0.f;
+        // Gradient column of input i: OUT consecutive floats, fetched as float4s.
+        auto g_column = [&](int i, float (&g)[OUT]) {
+#pragma unroll
+            for (int o = 0; o < OUT; o += 4) {
+                const float4 t = *reinterpret_cast<const float4 *>(gm + i * OUT + o);
+                g[o] = t.x; g[o + 1] = t.y; g[o + 2] = t.z; g[o + 3] = t.w;
+            }
+        };
+        for (int i = 0; i < I; i++) {
+            Cols<V> y;
+            ld_cols<V>(cache + in_row[i] * D + col, y);
+            float g[OUT];
+            g_column(i, g);
+#pragma unroll
+            for (int o = 0; o < OUT; o++) {
                 if (o >= O) break;
-                float acc = 0.f;
-                for (int i = 0; i < I; i++) acc = fmaf(gm[o * MI + i], cache[in_row[i] * LD + k], acc);
-                md[o] = acc;
-            }
-            for (int i = 0; i < I; i++) {
-                float acc = 0.f;
-                for (int o = 0; o < O; o++) acc = fmaf(gm[o * MI + i], outs[o * LD + k], acc);
-                cache[in_row[i] * LD + k] += acc;
-            }
-            const uint32_t salt = mix32(key0 + step * 0x9E3779B9u + (uint32_t)k);
-            out_rows.add(out_word[0], k, md[0], mix32(salt ^ (uint32_t)out_word[0]));
-            out_rows.add(out_word[O - 1], k, md[O - 1], mix32(salt ^ (uint32_t)out_word[O - 1] ^ 0xA5A5u));
 #pragma unroll
-            for (int o = 1; o < 23; o++) {
-                if (o >= O - 1) break;
-                pool_cur[(uint64_t)out_slot[o] * D + k] += md[o];
+                for (int k = 0; k < V; k++) md[o].v[k] = fmaf(g[o], y.v[k], md[o].v[k]);
             }
         }
-        __syncthreads();
+        // ---- inputs += corr^T . outputs (dsgl.hpp:1303-1350), in input order ----
+        for (int i = 0; i < I; i++) {
+            Cols<V> acc;
+#pragma unroll
+            for (int k = 0; k < V; k++) acc.v[k] = 0.f;
+            float g[OUT];
+            g_column(i, g);
+#pragma unroll
+            for (int o = 0; o < OUT; o++) {
+                if (o >= O) break;
+#pragma unroll
+                for (int k = 0; k < V; k++) acc.v[k] = fmaf(g[o], x[o].v[k], acc.v[k]);
+            }
+            float *row = cache + in_row[i] * D + col;
+            Cols<V> c;
+            ld_cols<V>(row, c);
+#pragma unroll
+            for (int k = 0; k < V; k++) c.v[k] += acc.v[k];
+            st_cols<V>(row, c);
+        }
+        // Centre rows in order (centre 1, then centre 2), updated from their values
+        // staged at the start of the step; pool rows from registers.
+        {
+            const int32_t w1 = out_word[0];
+            out_rows.apply(w1, col, x[0], md[0], salt_of(w1, 0x77u));
+        }
+#pragma unroll
+        for (int o = 1; o < OUT; o++) {
+            if (o == O - 1) {
+                const int32_t w2 = out_word[o];
+                Cols<V> base = x[o];
+                if (w2 == out_word[0] && !out_rows.is_master(w2)) {
+                    // The same BF16 row as centre 1: continue from what was just stored.
+                    out_rows.load_old(w2, col, base);
+                }
+                out_rows.apply(w2, col, base, md[o], salt_of(w2, 0x78u));
+            } else if (o < O - 1) {
+                // x[o] holds this pool row as staged at the start of the step and
+                // only this worker writes its columns, so no re-load is needed.
+#pragma unroll
+                for (int k = 0; k < V; k++) x[o].v[k] += md[o].v[k];
+                st_cols<V>(pool_cur + (uint64_t)out_slot[o] * D + col, x[o]);
+            }
+        }
 
         // ---- advance; write back finished sentences and spent pools (dsgl.hpp:1398-1424) ----
         step++;
-        const int p0 = s_pos[0] + 1, p1 = s_pos[1] + 1;
-        const bool end0 = p0 >= s_len[0], end1 = p1 >= s_len[1];
-        if (end0) { flush_sentence(0); train_sen_num++; }
-        if (end1) { flush_sentence(1); train_sen_num++; }
+        pos[0]++;
+        pos[1]++;
+        for (int s = 0; s < 2; s++)
+            if (pos[s] >= len[s]) {
+                flush_sentence(s);
+                len[s] = 0;
+                train_sen_num++;
+            }
         if (train_sen_num >= 2) {
             flush_pool();
             change_neg = true;
             pool_loaded = false;
             train_sen_num = 0;
         }
-        __syncthreads();
-        if (tid == 0) {
-            s_pos[0] = p0;
-            s_pos[1] = p1;
-            if (end0) s_len[0] = 0;
-            if (end1) s_len[1] = 0;
-        }
+        __syncthreads();   // bookkeeping arrays are rewritten next step
     }
     // Slice exhausted: keep the updates of the sentence still in flight and of
     // the pool (dsgl drops them; here they are written back).
-    __syncthreads();
     for (int s = 0; s < 2; s++)
-        if (s_len[s] != 0) flush_sentence(s);
+        if (len[s] != 0) flush_sentence(s);
     if (pool_loaded) flush_pool();
     if (tid == 0) {
-        atomicAdd(&a.stats[0], s_words);
-        atomicAdd(&a.stats[1], s_trained);
-        atomicAdd(&a.stats[2], s_pairs);
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
     }
 }
 
-static size_t mb_smem_bytes(int d, int max_out, int max_in, uint32_t pool_cap) {
-    const size_t ld = (size_t)d + 1;
-    size_t f = 2 * kMbMaxSent * ld + (size_t)max_out * ld + (size_t)max_out * max_in;
-    size_t i = 6 * kMbMaxSent + (size_t)max_in + 3 * (size_t)max_out + 2 * (size_t)pool_cap;
-    return f * 4 + i * 4;
+// Launch geometry shared by both entry points.
+struct MbPlan {
+    MbArgs m{};
+    int out = 8;
+    int threads = 32;
+    int per_sm = 0;
+};
+
+template <int D, int OUT>
+static int mb_setup(MbPlan &plan) {
+    plan.threads = 32 * mb_warps(D);
+    DG_CUDA(cudaFuncSetAttribute(sgns_mb_kernel<D, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)plan.m.smem));
+    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&plan.per_sm, sgns_mb_kernel<D, OUT>, plan.threads,
+                                                          plan.m.smem));
+    return DG_OK;
+}
+
+template <int OUT>
+static int mb_setup_d(int d, MbPlan &plan) {
+    switch (d) {
+    case 32: return mb_setup<32, OUT>(plan);
+    case 64: return mb_setup<64, OUT>(plan);
+    case 128: return mb_setup<128, OUT>(plan);
+    default: return mb_setup<256, OUT>(plan);
+    }
+}
+
+static int mb_plan(int d, int negative, int window, MbPlan &plan) {
+    DG_CHECK(d == 32 || d == 64 || d == 128 || d == 256, DG_ERR_ARG,
+             "size %d not supported in minibatch mode (32, 64, 128, 256)", d);
+    DG_CHECK(negative >= 0 && negative <= 14, DG_ERR_ARG, "minibatch mode supports negative <= 14 (got %d)", negative);
+    DG_CHECK(window >= 1 && window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", window);
+    plan.out = negative + 2 <= 8 ? 8 : 16;
+    MbArgs &m = plan.m;
+    m.pool_cap = (uint32_t)kMbMaxSent * (uint32_t)std::max(negative, 1);
+    m.max_in = 4 * window;
+    m.scratch_stride = (uint64_t)m.pool_cap * d * 2 + 2ull * kMbMaxSent * d;
+    m.smem = mb_smem_bytes(d, plan.out, m.max_in, m.pool_cap);
+    int rc = plan.out == 8 ? mb_setup_d<8>(d, plan) : mb_setup_d<16>(d, plan);
+    if (rc) return rc;
+    DG_CHECK(plan.per_sm >= 1, DG_ERR_ARG, "minibatch kernel does not fit (%u bytes of shared memory)", m.smem);
+    return DG_OK;
+}
+
+template <int OUT>
+static void mb_launch_out(int d, unsigned workers, const MbPlan &plan, cudaStream_t s, const SgnsArgs &a,
+                          const WalkSet &ws, const MbArgs &m) {
+    const size_t smem = plan.m.smem;
+    switch (d) {
+    case 32: sgns_mb_kernel<32, OUT><<<workers, 32 * mb_warps(32), smem, s>>>(a, ws, m); break;
+    case 64: sgns_mb_kernel<64, OUT><<<workers, 32 * mb_warps(64), smem, s>>>(a, ws, m); break;
+    case 128: sgns_mb_kernel<128, OUT><<<workers, 32 * mb_warps(128), smem, s>>>(a, ws, m); break;
+    default: sgns_mb_kernel<256, OUT><<<workers, 32 * mb_warps(256), smem, s>>>(a, ws, m); break;
+    }
+}
+
+static void mb_launch(int d, unsigned workers, const MbPlan &plan, cudaStream_t s, const SgnsArgs &a,
+                      const WalkSet &ws, const MbArgs &m) {
+    if (plan.out == 8) mb_launch_out<8>(d, workers, plan, s, a, ws, m);
+    else mb_launch_out<16>(d, workers, plan, s, a, ws, m);
+    dg::note_launch();
 }
 
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    const int d = s->p.size;
-    DG_CHECK(d <= 256, DG_ERR_ARG, "minibatch mode supports size <= 256 (got %d)", d);
-    DG_CHECK(a.negative <= 22, DG_ERR_ARG, "minibatch mode supports negative <= 22 (got %d)", a.negative);
-    MbArgs m{};
-    m.pool_cap = (uint32_t)kMbMaxSent * (uint32_t)std::max(a.negative, 1);
-    m.max_out = a.negative + 2;
-    m.max_in = 4 * a.window;
-    const size_t smem = mb_smem_bytes(d, m.max_out, m.max_in, m.pool_cap);
-    m.scratch_stride = (uint64_t)m.pool_cap * d * 2 + 2ull * kMbMaxSent * d;
-    int per_sm = 1;
-    auto setup = [&](auto kern) -> int {
-        DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMbThreads, smem));
-        return DG_OK;
-    };
-    int rc = DG_OK;
-    switch (d) {
-    case 32: rc = setup(sgns_mb_kernel<32>); break;
-    case 64: rc = setup(sgns_mb_kernel<64>); break;
-    case 128: rc = setup(sgns_mb_kernel<128>); break;
-    case 256: rc = setup(sgns_mb_kernel<256>); break;
-    default: return dg::fail(DG_ERR_ARG, "size %d not supported in minibatch mode", d);
-    }
+    MbPlan plan;
+    int rc = mb_plan(s->p.size, a.negative, a.window, plan);
     if (rc) return rc;
-    DG_CHECK(per_sm >= 1, DG_ERR_ARG, "minibatch kernel does not fit (%zu bytes of shared memory)", smem);
-    uint32_t workers = a.deterministic ? 1u : (uint32_t)(dg::sm_count(s->device) * per_sm);
+    uint32_t workers = a.deterministic ? 1u : (uint32_t)(dg::sm_count(s->device) * plan.per_sm);
     if (workers > ws.n_walks / 2 + 1) workers = std::max(1u, ws.n_walks / 2);
-    const uint64_t need = m.scratch_stride * workers;
+    const uint64_t need = plan.m.scratch_stride * workers;
     if (s->scratch.n < need) DG_CUDA(s->scratch.alloc(need));
+    MbArgs m = plan.m;
     m.scratch = s->scratch.p;
-    switch (d) {
-    case 32: sgns_mb_kernel<32><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
-    case 64: sgns_mb_kernel<64><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
-    case 128: sgns_mb_kernel<128><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
-    case 256: sgns_mb_kernel<256><<<workers, kMbThreads, smem, s->stream>>>(a, ws, m); break;
-    }
-    dg::note_launch();
+    mb_launch(s->p.size, workers, plan, s->stream, a, ws, m);
     DG_CUDA(cudaGetLastError());
     return DG_OK;
 }
@@ -514,46 +744,24 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
              "dg_sgns_minibatch_train_noalloc: walk or table pointer is NULL");
     DG_CHECK(x->in_bf16 && x->out_bf16 && (x->n_master == 0 || (x->in_master && x->out_master)), DG_ERR_ARG,
              "dg_sgns_minibatch_train_noalloc: row pointer is NULL");
-    const int d = x->size;
-    DG_CHECK(d == 32 || d == 64 || d == 128 || d == 256, DG_ERR_ARG, "size %d not supported (32, 64, 128, 256)", d);
-    DG_CHECK(x->window >= 1 && x->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", x->window);
-    DG_CHECK(x->negative >= 0 && x->negative <= 22, DG_ERR_ARG, "negative %d out of range [0, 22]", x->negative);
     DG_CHECK(x->vocab_size > 0 && x->table_size > 0 && x->table_size < (1ull << 32), DG_ERR_ARG,
              "empty vocabulary or unigram table");
+    const int d = x->size;
+    MbPlan plan;
+    int rc = mb_plan(d, x->negative, x->window, plan);
+    if (rc) return rc;
     int device = 0;
     DG_CUDA(cudaGetDevice(&device));
     float *scratch = nullptr;
     unsigned long long *stats = nullptr;
-    int rc = noalloc_pointers(device, &scratch, &stats);
+    rc = noalloc_pointers(device, &scratch, &stats);
     if (rc) return rc;
-
-    MbArgs m{};
-    m.pool_cap = (uint32_t)kMbMaxSent * (uint32_t)std::max(x->negative, 1);
-    m.max_out = x->negative + 2;
-    m.max_in = 4 * x->window;
-    m.scratch_stride = (uint64_t)m.pool_cap * d * 2 + 2ull * kMbMaxSent * d;
-    m.scratch = scratch;
-    const uint64_t per_worker = m.scratch_stride * sizeof(float);
+    const uint64_t per_worker = plan.m.scratch_stride * sizeof(float);
     const uint64_t max_workers = kNoAllocScratchBytes / per_worker;
     DG_CHECK(max_workers >= 1, DG_ERR_ARG,
              "size %d with negative %d needs %llu bytes of scratch per worker, more than the %zu-byte static area",
              d, x->negative, (unsigned long long)per_worker, kNoAllocScratchBytes);
-    const size_t smem = mb_smem_bytes(d, m.max_out, m.max_in, m.pool_cap);
-    int per_sm = 1;
-    auto setup = [&](auto kern) -> int {
-        DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, kMbThreads, smem));
-        return DG_OK;
-    };
-    switch (d) {
-    case 32: rc = setup(sgns_mb_kernel<32>); break;
-    case 64: rc = setup(sgns_mb_kernel<64>); break;
-    case 128: rc = setup(sgns_mb_kernel<128>); break;
-    default: rc = setup(sgns_mb_kernel<256>); break;
-    }
-    if (rc) return rc;
-    DG_CHECK(per_sm >= 1, DG_ERR_ARG, "minibatch kernel does not fit (%zu bytes of shared memory)", smem);
-    uint64_t workers = x->deterministic ? 1 : (uint64_t)dg::sm_count(device) * per_sm;
+    uint64_t workers = x->deterministic ? 1 : (uint64_t)dg::sm_count(device) * plan.per_sm;
     workers = std::min<uint64_t>(workers, max_workers);
     if (workers > x->n_walks / 2 + 1) workers = std::max<uint64_t>(1, x->n_walks / 2);
 
@@ -582,16 +790,12 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
     ws.verts = x->verts;
     ws.offsets = x->offsets;
     ws.n_walks = x->n_walks;
+    MbArgs m = plan.m;
+    m.scratch = scratch;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     DG_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s));  // counters start at zero every call
-    switch (d) {
-    case 32: sgns_mb_kernel<32><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
-    case 64: sgns_mb_kernel<64><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
-    case 128: sgns_mb_kernel<128><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
-    default: sgns_mb_kernel<256><<<(unsigned)workers, kMbThreads, smem, s>>>(a, ws, m); break;
-    }
-    dg::note_launch();
+    mb_launch(d, (unsigned)workers, plan, s, a, ws, m);
     DG_CUDA(cudaGetLastError());
     if (info) {
         unsigned long long st[4];

@@ -216,7 +216,7 @@ int dgo_sgns_plain(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_
 
 /* ------------------------------------------------------------ minibatch -- */
 
-#define MB_MAX_SENT 64
+#define MB_MAX_SENT 32
 #define MB_WIN_TAG 0x4D425749u
 #define MB_POOL_TAG 0x4D42504Fu
 

@@ -10,9 +10,10 @@
  *    product is a per-lane fused multiply-add chain followed by an xor butterfly
  *    over 16, 8, 4, 2, 1 lanes, lane 0's value used by all; neu1e and the
  *    positive row use fused multiply-adds, negative rows add a rounded g*x;
- *  - minibatch: each dot product is one fused multiply-add chain over the
- *    dimensions; output gradients chain over inputs, input gradients over
- *    outputs; cache write-back adds (current - loaded).
+ *  - minibatch: the row is split into 4 column blocks (d >= 128; d / 32 blocks
+ *    below), each reduced like a plain-rule dot, block sums added in order;
+ *    output gradients chain over inputs, input gradients over outputs; cache
+ *    write-back adds (current - loaded).
  * Compiled with -ffp-contract=off, so only the explicit fmaf calls fuse.
  */
 #include "dg_oracle.h"
@@ -24,7 +25,7 @@
 
 #define EXP_TABLE_SIZE 1000
 #define MAX_EXP 6
-#define MB_MAX_SENT 64
+#define MB_MAX_SENT 32
 #define MB_WIN_TAG 0x4D425749u
 #define MB_POOL_TAG 0x4D42504Fu
 
@@ -58,6 +59,17 @@ static float warp_dot(const float *a, const float *b, int d) {
         memcpy(p, q, sizeof(p));
     }
     return p[0];
+}
+
+/* Minibatch corr dot: the row's columns are split into nw contiguous blocks of
+ * 64 (nw = d / 64; one block for d = 32), one warp each; every block is reduced
+ * as warp_dot reduces a row, and the block sums are added in block order. */
+static float split_dot(const float *a, const float *b, int d) {
+    const int nw = d >= 64 ? d / 64 : 1;
+    const int blk = d / nw;
+    float f = warp_dot(a, b, blk);
+    for (int w = 1; w < nw; w++) f += warp_dot(a + w * blk, b + w * blk, blk);
+    return f;
 }
 
 int dgo_sgns_plain_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
@@ -242,8 +254,7 @@ int dgo_sgns_minibatch_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const
         for (int o = 0; o < O; o++)
             for (int i = 0; i < I; i++) {
                 const float *x = outs + (size_t)o * d, *y = ROW(i);
-                float f = 0.f;
-                for (int k = 0; k < d; k++) f = fmaf(x[k], y[k], f);
+                const float f = split_dot(x, y, d);
                 int label = i < first ? (o == 0) : (o == O - 1);
                 gm[o * MI + i] = grad32(f, label, c->exp_table, alpha) * (float)out_meta[o];
             }

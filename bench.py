@@ -362,6 +362,90 @@ def run_ours(args, rank, world, local, pg):
     return line
 
 
+AUC_HP = dict(size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1, min_count=0)
+
+
+def auc_split(workload: str):
+    """The workload's graph with 10% of its edges held out (gtrain.cpp's rule) plus
+    as many non-edges: (v_num, train_edges, pairs, labels)."""
+    from distger import graphgen, lp
+    cfg = graphgen.CONFIGS[workload]
+    edges = graphgen.chung_lu(**cfg)
+    train, pairs, labels = lp.split(edges, cfg["n"], frac=0.1, seed=2)
+    return cfg["n"], train, pairs, labels
+
+
+def run_auc_ours(args, local):
+    """The whole embedding job (30 walk rounds streamed into SGNS) for each trainer
+    form on the held-out split; one JSON line per form with its AUC and rates."""
+    import torch
+    import distger
+    from distger import lp
+    from distger.embed import embed
+    torch.cuda.set_device(local)
+    v, train, pairs, labels = auc_split(args.workload)
+    runs = [(m, 0) for m in args.auc_modes.split(",")]
+    if args.workers:
+        runs = [(m, int(w)) for m in args.auc_modes.split(",") for w in args.workers.split(",")]
+    for mode, workers in runs:
+        graph = distger.Graph(v, edges=train, make_undirected=True, device=local)
+        clocks = Clocks(local)
+        clocks.start()
+        res = embed(graph, mode=mode, seed=args.seed, workers=workers, device=local, **AUC_HP)
+        clk = clocks.stop()
+        graph.close()
+        m = lp.evaluate(res["embedding"], pairs, labels)
+        print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
+                          "sgns_form": mode, "dtype": "f32" if mode == "plain" else "bf16", "workers": workers,
+                          "auc": m["auc"],
+                          "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
+                          "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
+                          "walk_steps_per_s": res["walk_steps_per_s"], "sgns_words_per_s": res["words_per_s"],
+                          "footprints": res["footprints"], "words": res["words"], "clocks": clk,
+                          "config": dict(AUC_HP, split="10% edges held out + equal uniform non-edges, seed 2",
+                                         walkers_per_round=v, min_L=20, min_R=5, lr="ExponentialDecayLR(alpha, 0.1)")}),
+              flush=True)
+
+
+def run_auc_reference(args):
+    """The reference walk engine + dsgl (oracle/_ref/ref_embed) on the same split,
+    all 30 rounds and the whole corpus, embedding scored by the same AUC code."""
+    import dgoracle
+    from distger import graphgen, lp
+    exe = os.path.join(dgoracle.HERE, "_ref", "ref_embed")
+    if not os.path.exists(exe):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_embed not built"}))
+        return
+    v, train, pairs, labels = auc_split(args.workload)
+    cores = os.cpu_count() or 1
+    with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
+        path = os.path.join(tmp, "g.bin")
+        graphgen.write_edges(path, train)
+        emb_path = os.path.join(tmp, "emb.txt")
+        cmd = [exe, "-g", path, "-v", str(v), "-w", str(v), "--min_L", "20", "--min_R", "5", "--make-undirected",
+               "-t", str(max(1, cores - 1)), "-o", os.path.join(tmp, "w"), "-size", "128", "-window", "10",
+               "-negative", "5", "-sample", "1e-3", "-alpha", "0.01", "-iter", "1", "-min-count", "0",
+               "-threads", str(cores), "-debug", "0", "-eoutput", emb_path]
+        t0 = time.perf_counter()
+        out = subprocess.run(cmd, capture_output=True, text=True, timeout=args.ref_timeout).stdout
+        wall = time.perf_counter() - t0
+        kv = {}
+        for line in out.splitlines():
+            if line.startswith("ref_embed"):
+                kv = dict(x.split("=") for x in line.split()[1:])
+        emb = lp.read_embedding_text(emb_path, v)
+    m = lp.evaluate(emb, pairs, labels)
+    walk_s, sgns_s = float(kv.get("walk_s", "nan")), float(kv.get("sgns_s", "nan"))
+    fp, walks, words = int(kv.get("footprints", 0)), int(kv.get("walks", 0)), int(kv.get("sgns_words", 0))
+    print(json.dumps({"metric": "link-prediction AUC", "impl": "reference", "workload": args.workload,
+                      "sgns_form": "dsgl", "dtype": "f32", "auc": m["auc"], "auc_cosine": m["auc_cosine"],
+                      "test_pairs": int(labels.size), "rounds": int(kv.get("rounds", 0)), "walk_s": walk_s,
+                      "sgns_s": sgns_s, "embed_wall_s": wall, "walk_steps_per_s": (fp - walks) / walk_s,
+                      "sgns_words_per_s": words / sgns_s, "footprints": fp, "words": words, "cores": cores,
+                      "config": dict(AUC_HP, split="10% edges held out + equal uniform non-edges, seed 2",
+                                     walkers_per_round=v, min_L=20, min_R=5)}), flush=True)
+
+
 def run_profile_case(args, local):
     """A small case of one kernel for ncu: the YouTube-shaped graph and trainer
     (rows larger than L2), one walk round of --profile-walks walkers, then one
@@ -403,9 +487,24 @@ def main():
     ap.add_argument("--mode", choices=["plain", "minibatch"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
+    ap.add_argument("--auc", action="store_true",
+                    help="run the whole embedding job on a 10%%-held-out split and print link-prediction AUC lines")
+    ap.add_argument("--workload", choices=["c1_small", "c2_youtube", "c3_livejournal"], default="c1_small",
+                    help="graph of the --auc run")
+    ap.add_argument("--auc-modes", default="plain,minibatch")
+    ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--tmpdir", default=None)
+    ap.add_argument("--ref-timeout", type=int, default=7200)
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.auc:
+        if args.impl == "reference":
+            run_auc_reference(args)
+        else:
+            run_auc_ours(args, int(os.environ.get("LOCAL_RANK", "0")))
         return
     rank, world, local, pg = dist_init()
     try:

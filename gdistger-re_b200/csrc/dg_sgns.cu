@@ -459,15 +459,21 @@ int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
         return std::max(per_sm, 1);
     };
     if (!s->p.deterministic) threads = kPlainThreads;
+    // An explicit worker count (warps) lowers the resident grid, never raises it.
+    auto cap = [&](int resident) {
+        if (s->p.workers == 0) return resident;
+        const int want = (int)((s->p.workers + kPlainThreads / 32 - 1) / (kPlainThreads / 32));
+        return std::max(1, std::min(resident, want));
+    };
     const bool fast = a.negative <= kFastNeg;
     switch (vec) {
 #define DG_PLAIN_CASE(V)                                                                             \
     case V:                                                                                          \
         if (fast) {                                                                                  \
-            if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_kernel<V>);   \
+            if (!s->p.deterministic) blocks = cap(dg::sm_count(s->device) * occ(sgns_plain_kernel<V>)); \
             sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                          \
         } else {                                                                                     \
-            if (!s->p.deterministic) blocks = dg::sm_count(s->device) * occ(sgns_plain_seq_kernel<V>); \
+            if (!s->p.deterministic) blocks = cap(dg::sm_count(s->device) * occ(sgns_plain_seq_kernel<V>)); \
             sgns_plain_seq_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                      \
         }                                                                                            \
         dg::note_launch();                                                                           \
@@ -556,6 +562,7 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     s->vocab_size = (uint32_t)s->vocab_ids.size();
     std::vector<uint32_t> thr;
     keep_thresholds(s->vocab_cn, p->sample, s->train_words, p->mode == DG_SGNS_MINIBATCH, thr);
+    if (p->mode == DG_SGNS_MINIBATCH) s->mb_workers = dgs::mb_worker_bound(s->vocab_cn, thr, p->negative);
     std::vector<int32_t> table;
     unigram_table(s->vocab_cn, s->p.table_size, table);
     std::vector<float> et;
@@ -754,6 +761,7 @@ extern "C" int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info) {
     DG_CHECK(s && info, DG_ERR_ARG, "dg_sgns_get_info: NULL argument");
     info->vocab_size = s->vocab_size;
     info->master_rows = s->n_master;
+    info->workers = s->p.workers ? s->p.workers : s->mb_workers;
     info->train_words = s->train_words;
     info->table_size = s->p.table_size;
     info->device_bytes = s->v2w.bytes() + s->keep_thr.bytes() + s->table.bytes() + s->exp_table.bytes() +

@@ -67,6 +67,10 @@ struct SgnsArgs {
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 
+// Concurrency bound of the minibatch form from the vocabulary (counts in
+// vocabulary order, subsampling keep thresholds out of 65536).
+uint32_t mb_worker_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int negative);
+
 }  // namespace dgs
 
 struct dg_sgns {
@@ -76,6 +80,7 @@ struct dg_sgns {
     uint32_t v_num = 0;
     uint32_t vocab_size = 0;
     uint32_t n_master = 0;
+    uint32_t mb_workers = 0;           // minibatch form: staleness bound on concurrent workers
     uint64_t train_words = 0;
     uint32_t pass = 0;
     std::vector<uint32_t> vocab_ids, vocab_cn;

@@ -32,6 +32,7 @@
 #include "dg_sgns.h"
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 namespace dgs {
@@ -671,11 +672,47 @@ static void mb_launch(int d, unsigned workers, const MbPlan &plan, cudaStream_t 
     dg::note_launch();
 }
 
+// Every worker trains on snapshot copies (its negative pool, its two sentences)
+// and writes them back as deltas, so a row held by k workers at once receives k
+// deltas computed from one stale value: the hottest row's effective step grows
+// with the number of workers holding it.  On the 10,000-vertex power-law graph
+// (hottest row in 64% of pools) about 190 concurrent holders trained stably and
+// about 380 diverged (rows grew until sigmoid saturated, link-prediction AUC fell
+// from 0.71 to 0.45).  The bound keeps the expected number of holders of the
+// hottest input row and of the hottest output row at kMbMaxHolders.
+constexpr double kMbMaxHolders = 128.0;
+
+uint32_t mb_worker_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int negative) {
+    if (cn.empty()) return 1;
+    // Negatives: unigram^0.75 (word2vec.cu:141-160); pool of kMbMaxSent x negative draws.
+    double z = 0.0, top = 0.0;
+    for (uint32_t c : cn) {
+        const double p = std::pow((double)c, 0.75);
+        z += p;
+        top = std::max(top, p);
+    }
+    const double p_neg = z > 0 ? top / z : 0.0;
+    const double hold_out = 1.0 - std::pow(1.0 - p_neg, (double)kMbMaxSent * std::max(negative, 1));
+    // Inputs: token frequency after subsampling; two sentences of kMbMaxSent tokens.
+    double kept = 0.0, kept_top = 0.0;
+    for (size_t w = 0; w < cn.size(); w++) {
+        const double k = (double)cn[w] * std::min(1.0, keep_thr[w] / 65536.0);
+        kept += k;
+        kept_top = std::max(kept_top, k);
+    }
+    const double p_tok = kept > 0 ? kept_top / kept : 0.0;
+    const double hold_in = 1.0 - std::pow(1.0 - p_tok, 2.0 * kMbMaxSent);
+    const double hold = std::max(hold_out, hold_in);
+    if (hold <= 0.0) return 0xFFFFFFFFu;
+    return (uint32_t)std::max(1.0, std::min(4.0e9, std::floor(kMbMaxHolders / hold)));
+}
+
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     MbPlan plan;
     int rc = mb_plan(s->p.size, a.negative, a.window, plan);
     if (rc) return rc;
     uint32_t workers = a.deterministic ? 1u : (uint32_t)(dg::sm_count(s->device) * plan.per_sm);
+    if (!a.deterministic) workers = std::min(workers, s->p.workers ? s->p.workers : s->mb_workers);
     if (workers > ws.n_walks / 2 + 1) workers = std::max(1u, ws.n_walks / 2);
     const uint64_t need = plan.m.scratch_stride * workers;
     if (s->scratch.n < need) DG_CUDA(s->scratch.alloc(need));
@@ -763,6 +800,7 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
              d, x->negative, (unsigned long long)per_worker, kNoAllocScratchBytes);
     uint64_t workers = x->deterministic ? 1 : (uint64_t)dg::sm_count(device) * plan.per_sm;
     workers = std::min<uint64_t>(workers, max_workers);
+    if (!x->deterministic && x->workers) workers = std::min<uint64_t>(workers, x->workers);
     if (workers > x->n_walks / 2 + 1) workers = std::max<uint64_t>(1, x->n_walks / 2);
 
     SgnsArgs a{};

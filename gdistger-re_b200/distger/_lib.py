@@ -44,7 +44,7 @@ class SgnsParams(C.Structure):
     _fields_ = [("size", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("batch_size", C.c_int),
                 ("sample", C.c_float), ("alpha", C.c_float), ("iter", C.c_int), ("min_count", C.c_int),
                 ("mode", C.c_int), ("deterministic", C.c_int), ("seed", C.c_uint64),
-                ("table_size", C.c_uint64), ("master_rows", C.c_uint32)]
+                ("table_size", C.c_uint64), ("master_rows", C.c_uint32), ("workers", C.c_uint32)]
 
 
 class TrainInfo(C.Structure):
@@ -64,11 +64,12 @@ class MinibatchArgs(C.Structure):
                 ("in_bf16", C.c_void_p), ("out_bf16", C.c_void_p), ("in_master", C.c_void_p),
                 ("out_master", C.c_void_p), ("n_master", C.c_uint32), ("size", C.c_int), ("window", C.c_int),
                 ("negative", C.c_int), ("alpha", C.c_float), ("seed", C.c_uint64), ("pass_", C.c_uint32),
-                ("deterministic", C.c_int)]
+                ("deterministic", C.c_int), ("workers", C.c_uint32)]
 
 
 class SgnsInfo(C.Structure):
-    _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("train_words", C.c_uint64),
+    _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("workers", C.c_uint32),
+                ("train_words", C.c_uint64),
                 ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 

@@ -1,0 +1,245 @@
+// huge_walk: the embedding job of the reference's src/examples/huge_walk.cpp on one
+// GPU, over the distger C ABI (include/distger.h).
+//
+// Flow (huge_walk.cpp:19-62 + word2vec.cu TrainModel, word2vec.cu:1246-1297):
+// load the edge file into a device CSR, build the SGNS vocabulary from the
+// vertices' in+out degrees (huge_walk.cpp:40-44, word2vec.cu:791-809), then run
+// the walk rounds of WalkEngine::random_walk (walk.hpp:609-782: round 1 with
+// -w x --min_R walkers, then -w walkers per round, 30 rounds) and stream every
+// round's walks straight into the trainer with the round's learning rate from
+// the schedule (word2vec.cu:1279-1290 uses ExponentialDecayLR(alpha, 0.1)).  The
+// reference writes each round to ./out/tmp-0-<r>.txt and reads it back; here the
+// walks stay in HBM and are written only when -o is given.
+//
+// Flags kept from the reference (option_helper.hpp:112-156, word2vec.cu:1546-1563,
+// dsgl.hpp:1496-1535):
+//   -g <edges.bin> -v <vertices> -w <walkers> [-o <walk prefix>] [--min_L n]
+//   [--min_R n] [--make-undirected] [-r rate: accepted, unused as in walk.hpp:616]
+//   -size -window -negative -batch-size -sample -alpha -iter -min-count
+//   -emb_output <file> (word2vec.cu) or -eoutput <file> (dsgl)
+//   -threads / -debug / -reuse-neg: accepted, no effect on one GPU
+//   -hs, -cbow, -binary: only 0 is supported (skip-gram, negative sampling, text)
+// Added for the GPU build:
+//   -mode plain|minibatch   trainer form (default plain = word2vec.cu semantics)
+//   -lr exp|fixed|cosine|step|custom   per-round schedule (default exp, decay 0.1)
+//   -rounds n               stop after round n (default 30)
+//   -train-from n           first round whose walks are trained (default 1;
+//                           word2vec.cu:1286 starts at round 3)
+//   -seed s  -device d  -deterministic 0|1  -master-rows n  -table-size n  -max-len n
+//   -workers n              concurrent trainer workers (0 = automatic)
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "distger.h"
+#include "lr_scheduler.h"
+
+namespace {
+
+struct Options {
+    std::string graph, walk_prefix, emb_output, mode = "plain", lr = "exp";
+    uint32_t v_num = 0, walker_num = 0, min_len = 0, init_round = 0;
+    bool undirected = false;
+    int size = 100, window = 5, negative = 5, batch_size = 11, iter = 5, min_count = 5;
+    float sample = 1e-3f, alpha = 0.025f;
+    bool alpha_set = false;
+    int rounds = 30, train_from = 1, device = 0, deterministic = 0, max_len = 0;
+    uint64_t seed = 1;
+    uint32_t master_rows = 0, workers = 0;
+    uint64_t table_size = 0;
+};
+
+[[noreturn]] void die(const char *what) {
+    fprintf(stderr, "huge_walk: %s\n", what);
+    exit(2);
+}
+
+void check(int rc, const char *call) {
+    if (rc != DG_OK) {
+        fprintf(stderr, "huge_walk: %s failed (%d): %s\n", call, rc, dg_last_error());
+        exit(1);
+    }
+}
+
+Options parse(int argc, char **argv) {
+    Options o;
+    for (int i = 1; i < argc; i++) {
+        const std::string a = argv[i];
+        auto val = [&]() -> const char * {
+            if (i + 1 >= argc) die(("missing value for " + a).c_str());
+            return argv[++i];
+        };
+        auto u32 = [&]() { return static_cast<uint32_t>(strtoul(val(), nullptr, 10)); };
+        auto i32 = [&]() { return atoi(val()); };
+        if (a == "-g" || a == "--graph") o.graph = val();
+        else if (a == "-v" || a == "--vertex") o.v_num = u32();
+        else if (a == "-w" || a == "--walker") o.walker_num = u32();
+        else if (a == "-o" || a == "--output") o.walk_prefix = val();
+        else if (a == "--min_L") o.min_len = u32();
+        else if (a == "--min_R") o.init_round = u32();
+        else if (a == "--make-undirected") o.undirected = true;
+        else if (a == "-p" || a == "--partition") die("partition files split the graph across MPI ranks; one GPU holds it all");
+        else if (a == "-r" || a == "--rate") val();
+        else if (a == "-size") o.size = i32();
+        else if (a == "-window") o.window = i32();
+        else if (a == "-negative") o.negative = i32();
+        else if (a == "-batch-size") o.batch_size = i32();
+        else if (a == "-sample") o.sample = static_cast<float>(atof(val()));
+        else if (a == "-alpha") { o.alpha = static_cast<float>(atof(val())); o.alpha_set = true; }
+        else if (a == "-iter") o.iter = i32();
+        else if (a == "-min-count") o.min_count = i32();
+        else if (a == "-emb_output" || a == "-eoutput") o.emb_output = val();
+        else if (a == "-threads" || a == "-debug" || a == "-reuse-neg" || a == "-train" || a == "-disk" ||
+                 a == "-sync-period" || a == "-min-sync-words" || a == "-full-sync-times" || a == "-message-size")
+            val();
+        else if (a == "-hs" || a == "-cbow" || a == "-binary") {
+            if (atoi(val()) != 0) die((a + " 1 is not supported: skip-gram with negative sampling, text output").c_str());
+        }
+        else if (a == "-mode") o.mode = val();
+        else if (a == "-lr") o.lr = val();
+        else if (a == "-rounds") o.rounds = i32();
+        else if (a == "-train-from") o.train_from = i32();
+        else if (a == "-seed") o.seed = strtoull(val(), nullptr, 10);
+        else if (a == "-device") o.device = i32();
+        else if (a == "-deterministic") o.deterministic = i32();
+        else if (a == "-master-rows") o.master_rows = u32();
+        else if (a == "-table-size") o.table_size = strtoull(val(), nullptr, 10);
+        else if (a == "-max-len") o.max_len = i32();
+        else if (a == "-workers") o.workers = u32();
+        else die(("unknown flag " + a).c_str());
+    }
+    // option_helper.hpp asserts -v, -g, --min_L, --min_R and -w are present.
+    if (o.graph.empty() || o.v_num == 0 || o.walker_num == 0)
+        die("usage: huge_walk -g edges.bin -v V -w W [--min_L L] [--min_R R] [--make-undirected] [-o prefix] "
+            "[-size d -window k -negative n -batch-size b -sample s -alpha a -iter i -min-count c "
+            "-emb_output file] [-mode plain|minibatch]");
+    if (o.mode != "plain" && o.mode != "minibatch") die("-mode must be plain or minibatch");
+    if (o.rounds < 1 || o.rounds > 30) die("-rounds must be 1..30 (walk.hpp:740 stops after round 30)");
+    return o;
+}
+
+std::unique_ptr<dg_host::LR> make_lr(const Options &o) {
+    // word2vec.cu:1279 hard-codes ExponentialDecayLR(0.025, 0.1); -alpha sets its start here.
+    const float a0 = o.alpha_set ? o.alpha : 0.025f;
+    if (o.lr == "exp") return std::make_unique<dg_host::ExponentialDecayLR>(a0, 0.1f);
+    if (o.lr == "fixed") return std::make_unique<dg_host::FixedLR>(a0);
+    if (o.lr == "cosine") return std::make_unique<dg_host::CosineAnnealingLR>(a0, a0 * 1e-4f, o.rounds);
+    if (o.lr == "step") return std::make_unique<dg_host::StepDecayLR>(a0, 0.5f, 3);
+    if (o.lr == "custom") return std::make_unique<dg_host::CustomLR>(a0);
+    die("-lr must be exp, fixed, cosine, step or custom");
+}
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+    const Options o = parse(argc, argv);
+    const auto t_start = std::chrono::steady_clock::now();
+
+    dg_graph *g = nullptr;
+    check(dg_graph_create(o.graph.c_str(), o.v_num, o.undirected ? 1 : 0, o.device, &g), "dg_graph_create");
+    dg_graph_info gi{};
+    check(dg_graph_get_info(g, &gi), "dg_graph_get_info");
+    const double load_s = seconds_since(t_start);
+    printf("graph %s: %u vertices, %llu CSR entries, %.1f MB on device, load %.3f s\n", o.graph.c_str(), gi.v_num,
+           static_cast<unsigned long long>(gi.m), gi.device_bytes / 1e6, load_s);
+
+    // Vocabulary counts: in + out degree per vertex (huge_walk.cpp:40-44).
+    std::vector<uint32_t> out_deg(o.v_num), in_deg(o.v_num), counts(o.v_num);
+    check(dg_graph_copy_csr(g, nullptr, nullptr, nullptr, out_deg.data(), in_deg.data()), "dg_graph_copy_csr");
+    for (uint32_t v = 0; v < o.v_num; v++) counts[v] = out_deg[v] + in_deg[v];
+
+    dg_sgns_params sp{};
+    sp.size = o.size;
+    sp.window = o.window;
+    sp.negative = o.negative;
+    sp.batch_size = o.batch_size;
+    sp.sample = o.sample;
+    sp.alpha = o.alpha;
+    sp.iter = o.iter;
+    sp.min_count = o.min_count;
+    sp.mode = o.mode == "plain" ? DG_SGNS_PLAIN : DG_SGNS_MINIBATCH;
+    sp.deterministic = o.deterministic;
+    sp.seed = o.seed;
+    sp.table_size = o.table_size;
+    sp.master_rows = o.master_rows;
+    sp.workers = o.workers;
+    dg_sgns *s = nullptr;
+    check(dg_sgns_create(&sp, o.v_num, counts.data(), o.device, &s), "dg_sgns_create");
+    dg_sgns_info si{};
+    check(dg_sgns_get_info(s, &si), "dg_sgns_get_info");
+    printf("vocab %u rows, d=%d, mode %s, %u FP32 master rows, table %llu\n", si.vocab_size, o.size, o.mode.c_str(),
+           si.master_rows, static_cast<unsigned long long>(si.table_size));
+
+    dg_walk_params wp{};
+    wp.min_len = o.min_len ? o.min_len : 20;       // walk.hpp:404, set_minLength ignores 0
+    wp.init_round = o.init_round ? o.init_round : 5;  // walk.hpp:405, set_init_round ignores 0
+    wp.walker_num = o.walker_num;
+    wp.max_len = static_cast<uint32_t>(o.max_len);
+    wp.seed = o.seed;
+
+    auto lr = make_lr(o);
+    const auto t_embed = std::chrono::steady_clock::now();
+    double walk_ms = 0, train_ms = 0, device_ms = 0;
+    uint64_t steps = 0, footprints = 0, words = 0, pairs = 0;
+    for (int r = 1; r <= o.rounds; r++) {
+        dg_paths *keep = nullptr;
+        dg_paths **keep_arg = o.walk_prefix.empty() ? nullptr : &keep;
+        if (r >= o.train_from) {
+            const float alpha = lr->get_lr();
+            dg_pipeline_info pi{};
+            check(dg_pipeline_round(g, s, &wp, static_cast<uint32_t>(r), 0, alpha, &pi, keep_arg), "dg_pipeline_round");
+            walk_ms += pi.walk.walk_ms;
+            train_ms += pi.train.train_ms;
+            device_ms += pi.total_ms;
+            steps += pi.walk.steps;
+            footprints += pi.walk.footprints;
+            words += pi.train.words;
+            pairs += pi.train.pairs;
+            printf("round %d: walks %u steps %llu Delat RE %g alpha %.9g walk %.3f ms train %.3f ms (%llu words)\n", r,
+                   pi.walk.n_walks, static_cast<unsigned long long>(pi.walk.steps), std::fabs(pi.walk.delta_h), alpha,
+                   pi.walk.walk_ms, pi.train.train_ms, static_cast<unsigned long long>(pi.train.words));
+        } else {
+            dg_paths *p = nullptr;
+            check(dg_walk_run_round(g, &wp, static_cast<uint32_t>(r), 0, &p), "dg_walk_run_round");
+            dg_round_info ri{};
+            check(dg_paths_get_info(p, &ri), "dg_paths_get_info");
+            walk_ms += ri.walk_ms;
+            device_ms += ri.walk_ms;
+            steps += ri.steps;
+            footprints += ri.footprints;
+            printf("round %d: walks %u steps %llu Delat RE %g (not trained) walk %.3f ms\n", r, ri.n_walks,
+                   static_cast<unsigned long long>(ri.steps), std::fabs(ri.delta_h), ri.walk_ms);
+            if (keep_arg) keep = p; else dg_paths_free(p);
+        }
+        if (keep) {
+            // walk.hpp:686: <prefix>-<rank>-<round>.txt, rank 0 of 1.
+            const std::string path = o.walk_prefix + "-0-" + std::to_string(r) + ".txt";
+            check(dg_paths_write_text(keep, path.c_str()), "dg_paths_write_text");
+            dg_paths_free(keep);
+        }
+    }
+    const double embed_s = seconds_since(t_embed);
+    if (!o.emb_output.empty()) check(dg_sgns_write_embedding(s, o.emb_output.c_str()), "dg_sgns_write_embedding");
+    const double total_s = seconds_since(t_start);
+
+    printf("walk-steps/s %.6e (walk kernels %.3f ms, %llu steps, %llu footprints)\n", steps / (walk_ms * 1e-3),
+           walk_ms, static_cast<unsigned long long>(steps), static_cast<unsigned long long>(footprints));
+    if (train_ms > 0)
+        printf("SGNS words/s %.6e (train kernels %.3f ms, %llu words, %llu pairs)\n", words / (train_ms * 1e-3),
+               train_ms, static_cast<unsigned long long>(words), static_cast<unsigned long long>(pairs));
+    printf("embed: device %.3f s, rounds wall %.3f s, end-to-end %.3f s (graph load %.3f s)\n", device_ms * 1e-3,
+           embed_s, total_s, load_s);
+    dg_sgns_free(s);
+    dg_graph_free(g);
+    return 0;
+}

@@ -147,6 +147,8 @@ typedef struct {
     uint64_t seed;
     uint64_t table_size; /* unigram table slots; 0 = 1e8 (word2vec.cu:66) */
     uint32_t master_rows; /* minibatch mode: hottest rows kept in FP32; 0 = 65536, >= vocabulary = all */
+    uint32_t workers;     /* concurrent trainer workers (warps in plain mode, CTAs in minibatch mode);
+                             0 = automatic; capped at what the GPU holds resident */
 } dg_sgns_params;
 
 /* Vocabulary from per-vertex counts (word2vec.cu:791-809 uses in+out degree,
@@ -188,6 +190,8 @@ DG_API int dg_sgns_copy_tables(const dg_sgns *s, int32_t *table, uint32_t *keep_
 typedef struct {
     uint32_t vocab_size;
     uint32_t master_rows;  /* rows held in FP32 (minibatch form) */
+    uint32_t workers;      /* worker bound: the params' workers, else (minibatch form) the automatic
+                              staleness bound; 0 = as many as the GPU holds */
     uint64_t train_words;  /* sum of the vocabulary counts */
     uint64_t table_size;
     uint64_t device_bytes;
@@ -238,11 +242,13 @@ typedef struct {
     float *out_master;         /* n_master x size FP32 output rows */
     uint32_t n_master;
     int size;                  /* 32, 64, 128 or 256 */
-    int window, negative;      /* negative <= 22 */
+    int window, negative;      /* window <= 64, negative <= 14 */
     float alpha;
     uint64_t seed;
     uint32_t pass;             /* pass counter: one value per call, as dg_sgns_train_* count them */
     int deterministic;         /* 1: one worker, walks in order */
+    uint32_t workers;          /* concurrent workers; 0 = as many as fit.  dg_sgns_get_info reports the
+                                  staleness bound the handle path applies to the same vocabulary */
 } dg_sgns_minibatch_args;
 
 /* No counterpart in the reference.  The minibatch trainer (DG_SGNS_MINIBATCH)

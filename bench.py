@@ -396,8 +396,8 @@ def run_auc_ours(args, local):
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": mode, "dtype": "f32" if mode == "plain" else "bf16", "workers": workers,
-                          "auc": m["auc"],
+                          "sgns_form": mode, "dtype": "f32" if mode == "plain" else "bf16",
+                          "workers": workers or res["workers"], "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
                           "walk_steps_per_s": res["walk_steps_per_s"], "sgns_words_per_s": res["words_per_s"],

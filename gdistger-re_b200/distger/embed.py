@@ -79,6 +79,7 @@ def embed(graph: Graph, walker_num: int | None = None, mode: str = "plain", size
     t2 = time.perf_counter()
     emb = np.zeros((v_num, size), np.float32)
     emb[ids] = rows
+    acc["workers"] = sgns.workers
     sgns.close()
     acc.update(rounds=per_round, embedding=emb, rounds_wall_s=t2 - t1, wall_s=t2 - t0,
                walk_steps_per_s=acc["steps"] / (acc["walk_ms"] * 1e-3) if acc["walk_ms"] else 0.0,

@@ -10,8 +10,9 @@
  *    product is a per-lane fused multiply-add chain followed by an xor butterfly
  *    over 16, 8, 4, 2, 1 lanes, lane 0's value used by all; neu1e and the
  *    positive row use fused multiply-adds, negative rows add a rounded g*x;
- *  - minibatch: the row is split into 4 column blocks (d >= 128; d / 32 blocks
- *    below), each reduced like a plain-rule dot, block sums added in order;
+ *  - minibatch: the row is split into d / 64 contiguous column blocks (one
+ *    block for d = 32), each reduced like a plain-rule dot over its block,
+ *    block sums added in block order;
  *    output gradients chain over inputs, input gradients over outputs; cache
  *    write-back adds (current - loaded).
  * Compiled with -ffp-contract=off, so only the explicit fmaf calls fuse.

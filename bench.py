@@ -387,16 +387,18 @@ def run_auc_ours(args, local):
     runs = [(m, 0) for m in args.auc_modes.split(",")]
     if args.workers:
         runs = [(m, int(w)) for m in args.auc_modes.split(",") for w in args.workers.split(",")]
-    for mode, workers in runs:
+    for form, workers in runs:
+        mode, _, variant = form.partition("-")          # plain, minibatch, plain-adjoint, minibatch-adjoint
         graph = distger.Graph(v, edges=train, make_undirected=True, device=local)
         clocks = Clocks(local)
         clocks.start()
-        res = embed(graph, mode=mode, seed=args.seed, workers=workers, device=local, **AUC_HP)
+        res = embed(graph, mode=mode, seed=args.seed, workers=workers, deterministic=2 if variant == "adjoint" else 0,
+                    device=local, **AUC_HP)
         clk = clocks.stop()
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": mode, "dtype": "f32" if mode == "plain" else "bf16",
+                          "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16",
                           "workers": workers or res["workers"], "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],

@@ -450,6 +450,113 @@ __global__ void __launch_bounds__(kPlainThreads) sgns_plain_seq_kernel(SgnsArgs 
     }
 }
 
+// ------------------------------------------------------- adjoint-mode pairs
+// The (context, centre) pairs the plain trainer forms in the same pass -- same
+// sentence (vocabulary lookup + subsampling draw), same window shrink b, contexts
+// at distance 1 .. window - b (word2vec.cu:328-340) -- laid out in walk order,
+// centre order, then left-to-right context order.  Counted first, written at
+// the scanned offsets second.
+constexpr int kPairThreads = 256;
+
+__device__ __forceinline__ uint32_t pair_span(uint32_t p, uint32_t wid, const SgnsArgs &a) {
+    return (uint32_t)a.window - philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % (uint32_t)a.window;
+}
+
+__global__ void __launch_bounds__(kPairThreads) adj_pair_count(SgnsArgs a, WalkSet ws, uint32_t *count) {
+    __shared__ int32_t sen_all[kPairThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    unsigned long long n_words = 0, n_trained = 0;
+    for (uint32_t walk = blockIdx.x * (kPairThreads / 32) + warp; walk < ws.n_walks;
+         walk += gridDim.x * (kPairThreads / 32)) {
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        uint32_t c = 0;
+        for (uint32_t p = lane; p < n; p += 32) {
+            const uint32_t span = pair_span(p, wid, a);
+            c += min(p, span) + min(n - 1 - p, span);
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (lane == 0) count[walk] = c;
+        __syncwarp();
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+    }
+}
+
+__global__ void __launch_bounds__(kPairThreads) adj_pair_fill(SgnsArgs a, WalkSet ws, const uint64_t *offs,
+                                                              uint32_t *inputs, uint32_t *outputs) {
+    __shared__ int32_t sen_all[kPairThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    for (uint32_t walk = blockIdx.x * (kPairThreads / 32) + warp; walk < ws.n_walks;
+         walk += gridDim.x * (kPairThreads / 32)) {
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        uint64_t base = offs[walk];
+        for (uint32_t p0 = 0; p0 < n; p0 += 32) {
+            const uint32_t p = p0 + lane;
+            uint32_t lo = 0, hi = 0, cnt = 0;
+            if (p < n) {
+                const uint32_t span = pair_span(p, wid, a);
+                lo = p - min(p, span);
+                hi = p + min(n - 1 - p, span);
+                cnt = hi - lo;
+            }
+            uint32_t incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+                if ((int)lane >= o) incl += t;
+            }
+            if (p < n) {
+                uint64_t q = base + incl - cnt;
+                for (uint32_t c = lo; c <= hi; c++) {
+                    if (c == p) continue;
+                    inputs[q] = (uint32_t)sen[c];
+                    outputs[q] = (uint32_t)sen[p];
+                    q++;
+                }
+            }
+            base += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        __syncwarp();
+    }
+}
+
+int adjoint_pairs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_pairs) {
+    n_pairs = 0;
+    if (ws.n_walks == 0) return DG_OK;
+    const unsigned blocks = (unsigned)std::min<uint64_t>((ws.n_walks + kPairThreads / 32 - 1) / (kPairThreads / 32),
+                                                         (uint64_t)dg::sm_count(s->device) * 8);
+    dg::DevArray<uint32_t> count;
+    DG_CUDA(count.alloc(ws.n_walks));
+    if (s->adj_offs.n < (size_t)ws.n_walks + 1) DG_CUDA(s->adj_offs.alloc((size_t)ws.n_walks + 1));
+    adj_pair_count<<<blocks, kPairThreads, 0, s->stream>>>(a, ws, count.p); dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    int rc = dg::exclusive_scan_u32_to_u64(count.p, s->adj_offs.p, ws.n_walks, s->stream);
+    if (rc) return rc;
+    DG_CUDA(cudaMemcpyAsync(&n_pairs, s->adj_offs.p + ws.n_walks, 8, cudaMemcpyDeviceToHost, s->stream));
+    DG_CUDA(cudaStreamSynchronize(s->stream));
+    if (s->adj_pin.n < n_pairs) {
+        DG_CUDA(s->adj_pin.alloc(n_pairs + n_pairs / 8));
+        DG_CUDA(s->adj_pout.alloc(n_pairs + n_pairs / 8));
+    }
+    if (n_pairs) {
+        adj_pair_fill<<<blocks, kPairThreads, 0, s->stream>>>(a, ws, s->adj_offs.p, s->adj_pin.p, s->adj_pout.p);
+        dg::note_launch();
+        DG_CUDA(cudaGetLastError());
+    }
+    return DG_OK;
+}
+
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     const int vec = s->p.size / 32;
     int blocks = 1, threads = 32;
@@ -531,7 +638,8 @@ dg_sgns::~dg_sgns() {
         cudaStreamSynchronize(stream);
         v2w.release(); keep_thr.release(); table.release(); exp_table.release();
         syn0.release(); syn1.release(); in_bf.release(); out_bf.release(); in_master.release(); out_master.release();
-        scratch.release(); queue.release(); stats.release();
+        scratch.release(); queue.release(); stats.release(); adj_in.release(); adj_out.release(); adj_flag.release();
+        adj_offs.release(); adj_pin.release(); adj_pout.release(); adj_neg.release();
         cudaStreamDestroy(stream);
     }
 }
@@ -548,6 +656,8 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CHECK(p->negative >= 0 && p->negative <= 64, DG_ERR_ARG, "negative %d out of range [0, 64]", p->negative);
     DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH, DG_ERR_ARG, "unknown mode %d", p->mode);
     DG_CHECK(p->iter >= 1, DG_ERR_ARG, "iter must be >= 1");
+    DG_CHECK(p->deterministic >= 0 && p->deterministic <= 2, DG_ERR_ARG, "deterministic must be 0, 1 or 2");
+    DG_CHECK(p->deterministic != 2 || p->negative <= 16, DG_ERR_ARG, "adjoint mode supports negative <= 16");
     int n_dev = 0;
     DG_CUDA(cudaGetDeviceCount(&n_dev));
     DG_CHECK(device >= 0 && device < n_dev, DG_ERR_ARG, "device %d out of range (%d)", device, n_dev);
@@ -563,6 +673,9 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     std::vector<uint32_t> thr;
     keep_thresholds(s->vocab_cn, p->sample, s->train_words, p->mode == DG_SGNS_MINIBATCH, thr);
     if (p->mode == DG_SGNS_MINIBATCH) s->mb_workers = dgs::mb_worker_bound(s->vocab_cn, thr, p->negative);
+    if (p->deterministic == 2)
+        s->adj_step_batches = dgs::adjoint_step_bound(
+            s->vocab_cn, thr, p->batch_size > 0 ? p->batch_size : 2 * p->window + 1, p->negative);
     std::vector<int32_t> table;
     unigram_table(s->vocab_cn, s->p.table_size, table);
     std::vector<float> et;
@@ -637,13 +750,23 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
     DG_CUDA(cudaMemsetAsync(s->stats.p, 0, 4 * sizeof(unsigned long long), s->stream));
     dg::EventTimer t;
     t.start(s->stream);
+    uint64_t adj_pairs = 0;
     for (int it = 0; it < s->p.iter; it++) {
         a.pass = s->pass++;
         DG_CUDA(cudaMemsetAsync(s->queue.p, 0, sizeof(uint32_t), s->stream));
-        int rc = s->p.mode == DG_SGNS_PLAIN ? launch_plain(s, a, ws) : launch_minibatch(s, a, ws);
+        int rc;
+        if (s->p.deterministic == 2) {
+            uint64_t np = 0;
+            rc = adjoint_train(s, a, ws, np);
+            adj_pairs += np;
+        } else {
+            rc = s->p.mode == DG_SGNS_PLAIN ? launch_plain(s, a, ws) : launch_minibatch(s, a, ws);
+        }
         if (rc) return rc;
     }
     t.stop(s->stream);
+    if (s->p.deterministic == 2)
+        DG_CUDA(cudaMemcpyAsync(s->stats.p + 2, &adj_pairs, 8, cudaMemcpyHostToDevice, s->stream));
     unsigned long long st[4];
     DG_CUDA(cudaMemcpyAsync(st, s->stats.p, sizeof(st), cudaMemcpyDeviceToHost, s->stream));
     DG_CUDA(cudaStreamSynchronize(s->stream));
@@ -761,7 +884,7 @@ extern "C" int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info) {
     DG_CHECK(s && info, DG_ERR_ARG, "dg_sgns_get_info: NULL argument");
     info->vocab_size = s->vocab_size;
     info->master_rows = s->n_master;
-    info->workers = s->p.workers ? s->p.workers : s->mb_workers;
+    info->workers = s->p.workers ? s->p.workers : s->p.deterministic == 2 ? s->adj_step_batches : s->mb_workers;
     info->train_words = s->train_words;
     info->table_size = s->p.table_size;
     info->device_bytes = s->v2w.bytes() + s->keep_thr.bytes() + s->table.bytes() + s->exp_table.bytes() +

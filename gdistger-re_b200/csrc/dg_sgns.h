@@ -71,6 +71,18 @@ int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 // vocabulary order, subsampling keep thresholds out of 65536).
 uint32_t mb_worker_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int negative);
 
+// Shares of the hottest row: among negative draws (unigram^0.75) and among
+// tokens kept by subsampling.
+void hot_row_shares(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, double &p_neg,
+                    double &p_tok);
+
+// Adjoint mode (deterministic = 2): gradient steps of the hand-written backward
+// kernel over the pass's pairs in shared-negative minibatches.
+int adjoint_pairs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_pairs);
+int adjoint_train(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_pairs);
+uint32_t adjoint_step_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int batch,
+                            int negative);
+
 }  // namespace dgs
 
 struct dg_sgns {
@@ -93,6 +105,12 @@ struct dg_sgns {
     dg::DevArray<__nv_bfloat16> in_bf, out_bf;
     dg::DevArray<float> in_master, out_master;
     dg::DevArray<float> scratch;       // minibatch form: per-worker negative pools and cache snapshots
+    dg::DevArray<unsigned long long> adj_in, adj_out;  // adjoint: fixed-point gradient sums (vocab x size)
+    dg::DevArray<unsigned int> adj_flag;
+    dg::DevArray<uint64_t> adj_offs;                    // adjoint mode: pair offsets per walk
+    dg::DevArray<uint32_t> adj_pin, adj_pout, adj_neg;  // adjoint mode: pairs and shared negatives
+    bool adj_dirty = false;                             // accumulators hold a finished gradient
+    uint32_t adj_step_batches = 1;                      // adjoint mode: minibatches per gradient step
     dg::DevArray<uint32_t> queue;
     dg::DevArray<unsigned long long> stats;
     ~dg_sgns();

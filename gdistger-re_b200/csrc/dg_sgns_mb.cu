@@ -682,25 +682,32 @@ static void mb_launch(int d, unsigned workers, const MbPlan &plan, cudaStream_t 
 // hottest input row and of the hottest output row at kMbMaxHolders.
 constexpr double kMbMaxHolders = 128.0;
 
-uint32_t mb_worker_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int negative) {
-    if (cn.empty()) return 1;
-    // Negatives: unigram^0.75 (word2vec.cu:141-160); pool of kMbMaxSent x negative draws.
+void hot_row_shares(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, double &p_neg,
+                    double &p_tok) {
+    // Negatives: unigram^0.75 (word2vec.cu:141-160).
     double z = 0.0, top = 0.0;
     for (uint32_t c : cn) {
         const double p = std::pow((double)c, 0.75);
         z += p;
         top = std::max(top, p);
     }
-    const double p_neg = z > 0 ? top / z : 0.0;
-    const double hold_out = 1.0 - std::pow(1.0 - p_neg, (double)kMbMaxSent * std::max(negative, 1));
-    // Inputs: token frequency after subsampling; two sentences of kMbMaxSent tokens.
+    p_neg = z > 0 ? top / z : 0.0;
+    // Tokens: frequency after subsampling.
     double kept = 0.0, kept_top = 0.0;
     for (size_t w = 0; w < cn.size(); w++) {
         const double k = (double)cn[w] * std::min(1.0, keep_thr[w] / 65536.0);
         kept += k;
         kept_top = std::max(kept_top, k);
     }
-    const double p_tok = kept > 0 ? kept_top / kept : 0.0;
+    p_tok = kept > 0 ? kept_top / kept : 0.0;
+}
+
+uint32_t mb_worker_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int negative) {
+    if (cn.empty()) return 1;
+    double p_neg, p_tok;
+    hot_row_shares(cn, keep_thr, p_neg, p_tok);
+    // A worker holds a pool of kMbMaxSent x negative draws and two sentences of kMbMaxSent tokens.
+    const double hold_out = 1.0 - std::pow(1.0 - p_neg, (double)kMbMaxSent * std::max(negative, 1));
     const double hold_in = 1.0 - std::pow(1.0 - p_tok, 2.0 * kMbMaxSent);
     const double hold = std::max(hold_out, hold_in);
     if (hold <= 0.0) return 0xFFFFFFFFu;

@@ -73,6 +73,12 @@ class SgnsInfo(C.Structure):
                 ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
 
 
+class SgnsPairs(C.Structure):
+    """dg_sgns_pairs: explicit shared-negative minibatches (host pointers)."""
+    _fields_ = [("inputs", C.c_void_p), ("outputs", C.c_void_p), ("negatives", C.c_void_p),
+                ("n_pairs", C.c_uint64), ("batch", C.c_uint32), ("negative", C.c_int)]
+
+
 _P = C.c_void_p
 _SIGS = {
     "dg_last_error": ([], C.c_char_p),
@@ -102,6 +108,8 @@ _SIGS = {
                            C.POINTER(PipelineInfo), C.POINTER(_P)], C.c_int),
     "dg_launch_count": ([], C.c_uint64),
     "dg_sgns_minibatch_train_noalloc": ([C.POINTER(MinibatchArgs), _P, C.POINTER(TrainInfo)], C.c_int),
+    "dg_sgns_loss_grad": ([_P, C.POINTER(SgnsPairs), C.POINTER(C.c_double), _P, _P], C.c_int),
+    "dg_sgns_adjoint_step": ([_P, C.POINTER(SgnsPairs), C.c_float, C.POINTER(C.c_double)], C.c_int),
 }
 
 _lib = None

@@ -91,6 +91,37 @@ class SGNS:
                                         et.ctypes.data))
         return {"table": table, "keep_thr": keep, "v2w": v2w, "exp_table": et}
 
+    @staticmethod
+    def _pairs(inputs, outputs, negatives, batch: int, negative: int):
+        inp = np.ascontiguousarray(inputs, dtype=np.uint32)
+        outp = np.ascontiguousarray(outputs, dtype=np.uint32)
+        neg = np.ascontiguousarray(negatives, dtype=np.uint32)
+        if inp.size != outp.size:
+            raise ValueError("inputs and outputs differ in length")
+        p = _lib.SgnsPairs(inputs=inp.ctypes.data if inp.size else None,
+                           outputs=outp.ctypes.data if outp.size else None,
+                           negatives=neg.ctypes.data if neg.size else None, n_pairs=inp.size, batch=batch,
+                           negative=negative)
+        return p, (inp, outp, neg)
+
+    def loss_grad(self, inputs, outputs, negatives, batch: int = 21, negative: int = 5, grad: bool = True):
+        """SGNS loss over explicit minibatches at the current rows and its gradient
+        (hand-written backward kernel, deterministic): (loss, grad_in, grad_out)."""
+        p, keep = self._pairs(inputs, outputs, negatives, batch, negative)
+        loss = C.c_double()
+        gi = np.empty((self.vocab_size, self.size), np.float32) if grad else None
+        go = np.empty((self.vocab_size, self.size), np.float32) if grad else None
+        check(lib().dg_sgns_loss_grad(self._h, C.byref(p), C.byref(loss), gi.ctypes.data if grad else None,
+                                      go.ctypes.data if grad else None))
+        return loss.value, gi, go
+
+    def adjoint_step(self, inputs, outputs, negatives, alpha: float, batch: int = 21, negative: int = 5) -> float:
+        """Deterministic step rows -= alpha * gradient; returns the loss before the step."""
+        p, keep = self._pairs(inputs, outputs, negatives, batch, negative)
+        loss = C.c_double()
+        check(lib().dg_sgns_adjoint_step(self._h, C.byref(p), C.c_float(alpha), C.byref(loss)))
+        return loss.value
+
     def write_embedding(self, path: str) -> None:
         check(lib().dg_sgns_write_embedding(self._h, path.encode()))
 

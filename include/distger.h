@@ -143,12 +143,18 @@ typedef struct {
     int iter;          /* -iter: passes over each round's walks */
     int min_count;     /* -min-count */
     int mode;          /* DG_SGNS_* */
-    int deterministic; /* 1: one warp trains everything in order (tests, replay) */
+    int deterministic; /* 0: Hogwild (fused updates, many workers);
+                          1: one warp / one worker trains everything in order (tests, replay);
+                          2: adjoint mode -- the plain trainer's pairs of each pass, in minibatches of
+                             batch_size pairs (0: 2*window+1) sharing `negative` (<= 16) negatives,
+                             trained by gradient steps of the hand-written backward kernel
+                             (dg_sgns_adjoint_step's rule); identical results at any GPU occupancy */
     uint64_t seed;
     uint64_t table_size; /* unigram table slots; 0 = 1e8 (word2vec.cu:66) */
     uint32_t master_rows; /* minibatch mode: hottest rows kept in FP32; 0 = 65536, >= vocabulary = all */
     uint32_t workers;     /* concurrent trainer workers (warps in plain mode, CTAs in minibatch mode);
-                             0 = automatic; capped at what the GPU holds resident */
+                             0 = automatic; capped at what the GPU holds resident.  Adjoint mode:
+                             minibatches per gradient step (0 = automatic bound) */
 } dg_sgns_params;
 
 /* Vocabulary from per-vertex counts (word2vec.cu:791-809 uses in+out degree,
@@ -202,6 +208,41 @@ DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *ou
 /* Embedding text: "%lld %lld\n" header then per row "%u " + size x "%lf " + "\n"
  * (word2vec.cu:1353-1362). */
 DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
+
+/* ------------------------------------------------- SGNS loss and adjoint */
+
+/* Explicit minibatches for the loss / gradient entry points: n_pairs (input,
+ * output) pairs in minibatches of `batch` consecutive pairs (the last one may be
+ * shorter), each minibatch sharing `negative` negative output rows -- dsgl's
+ * shared-negative minibatch (dsgl.hpp:1055-1156; batch 2*window+1 = 21).  Ids
+ * are vocabulary rows (0 .. vocab_size-1).  Host pointers. */
+typedef struct {
+    const uint32_t *inputs;     /* [n_pairs] input rows (the context word of a pair) */
+    const uint32_t *outputs;    /* [n_pairs] positive output rows (the centre word) */
+    const uint32_t *negatives;  /* [ceil(n_pairs / batch) * negative] */
+    uint64_t n_pairs;
+    uint32_t batch;             /* >= 1 */
+    int negative;               /* 0 .. 16 */
+} dg_sgns_pairs;
+
+/* The SGNS loss that word2vec.cu's skip_gram_kernel (word2vec.cu:305-399) and
+ * dsgl's minibatch update (dsgl.hpp:1241-1311) descend with fused Hogwild
+ * updates, evaluated at the trainer's current rows (FP32 rows in plain mode,
+ * BF16 rows + FP32 masters in minibatch mode):
+ *   L = sum_pairs softplus(-v_in . u_out) + sum_{minibatch negatives k} softplus(v_in . u_k)
+ * with the exact logistic sigmoid, and its gradient by a hand-written backward
+ * kernel.  loss: FP64 sum; grad_in / grad_out: vocab_size x size FP32 in
+ * vocabulary order (each may be NULL).  Deterministic: contributions are summed
+ * in 64-bit fixed point (2^-40 resolution), so equal inputs give bit-identical
+ * gradients whatever the thread schedule.  A contribution that is not finite or
+ * reaches 2^20 in magnitude is DG_ERR_ARG. */
+DG_API int dg_sgns_loss_grad(dg_sgns *s, const dg_sgns_pairs *pairs, double *loss, float *grad_in, float *grad_out);
+
+/* The deterministic training step that replaces the fused update: the gradient
+ * above at the current rows, then rows -= alpha * gradient for both tables,
+ * rounded to nearest in the rows' storage.  loss (may be NULL) is the loss
+ * before the step. */
+DG_API int dg_sgns_adjoint_step(dg_sgns *s, const dg_sgns_pairs *pairs, float alpha, double *loss);
 
 /* --------------------------------------------------------------- pipeline */
 

@@ -157,6 +157,12 @@ int dgo_sgns_plain_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uin
 int dgo_sgns_minibatch_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
                            float *syn0, float *syn1, dgo_sgns_stats *st);
 
+/* FP64 SGNS loss and gradient over explicit minibatches (dg_oracle_adjoint.c). */
+int dgo_sgns_loss_grad(const double *in, const double *out, int d, uint32_t vocab_size, const uint32_t *inputs,
+                       const uint32_t *outputs, const uint32_t *negatives, uint64_t n_pairs, uint32_t batch,
+                       int negative, int only_table, int64_t only_row, double *loss, double *grad_in,
+                       double *grad_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -98,6 +98,9 @@ def lib():
                                          C.c_void_p]
         L.dgo_sgns_minibatch_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                              C.c_void_p, C.c_void_p]
+        L.dgo_sgns_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
+                                         C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.c_int64,
+                                         C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -311,3 +314,26 @@ def entropy_table(max_sn: int) -> np.ndarray:
     out = np.empty(n, dtype=np.float64)
     lib().dgo_entropy_table(max_sn, out.ctypes.data)
     return out
+
+
+def sgns_loss_grad(in_rows: np.ndarray, out_rows: np.ndarray, inputs, outputs, negatives, batch: int,
+                   negative: int, grad: bool = True, only=None):
+    """FP64 SGNS loss (and gradient) over explicit minibatches (dg_oracle_adjoint.c).
+    only = (table, row) restricts the sum to the pairs whose terms depend on that row."""
+    a = np.ascontiguousarray(in_rows, dtype=np.float64)
+    b = np.ascontiguousarray(out_rows, dtype=np.float64)
+    vocab, d = a.shape
+    inp = np.ascontiguousarray(inputs, dtype=np.uint32)
+    outp = np.ascontiguousarray(outputs, dtype=np.uint32)
+    neg = np.ascontiguousarray(negatives, dtype=np.uint32)
+    loss = C.c_double()
+    gi = np.zeros((vocab, d)) if grad else None
+    go = np.zeros((vocab, d)) if grad else None
+    table, row = only if only is not None else (0, -1)
+    rc = lib().dgo_sgns_loss_grad(a.ctypes.data, b.ctypes.data, d, vocab, inp.ctypes.data, outp.ctypes.data,
+                                  neg.ctypes.data if neg.size else None, inp.size, batch, negative, table, row,
+                                  C.byref(loss), gi.ctypes.data if grad else None,
+                                  go.ctypes.data if grad else None)
+    if rc:
+        raise RuntimeError("dgo_sgns_loss_grad failed")
+    return loss.value, gi, go

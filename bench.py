@@ -48,6 +48,10 @@ WORKLOAD = {"graph": "youtube-shaped chung-lu", "vertices": 1_138_499, "undirect
 # Algorithmic bytes per unit (roofline section).
 BYTES_PER_PAIR_PLAIN = lambda d, n: 2 * (2 + n) * d * 4          # noqa: E731  context + 1+n targets, read+write
 BYTES_PER_DRAW, BYTES_PER_FOOTPRINT = 28, 4
+# Adjoint pass, per pair: rows read (input, positive output, negative/batch shared rows) at e bytes, the 8-byte
+# fixed-point accumulators read and written by the gradient kernel, then read and cleared by the step kernel,
+# which also reads and writes the row element.
+BYTES_PER_PAIR_ADJOINT = lambda d, n, b, e: (2 + n / b) * d * (3 * e + 32)   # noqa: E731
 
 
 def peaks():
@@ -234,7 +238,8 @@ def run_ours(args, rank, world, local, pg):
     counts = csr["out_deg"] + csr["in_deg"]              # word2vec vocabulary from degrees (huge_walk.cpp:43-46)
     mode = args.mode
     sgns = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
-                min_count=0, mode=mode, seed=1 + rank, device=local)
+                min_count=0, mode=mode, seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local)
+    form = mode + ("_adjoint" if args.adjoint else "")
     wp = _lib.WalkParams(min_len=20, init_round=10, walker_num=v_num, max_len=64, seed=2024 + rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
 
@@ -311,6 +316,9 @@ def run_ours(args, rank, world, local, pg):
     if train_ms >= walk_ms:
         kern = "sgns_plain" if mode == "plain" else "sgns_minibatch"
         alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else None
+        if args.adjoint:
+            kern = "sgns_adjoint pass (pair cut + gradient + step kernels)"
+            alg = pairs * BYTES_PER_PAIR_ADJOINT(128, 5, 21, 4 if mode == "plain" else 2)
         kms = train_ms
         per = traffic.get(kern, {}).get("dram_bytes_per_pair")
         tr = per * pairs / args.steps if per else None
@@ -348,8 +356,8 @@ def run_ours(args, rank, world, local, pg):
                 "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == "plain" else "bf16",
                 "data": "synthetic",
-                "config": dict(WORKLOAD, workload="c2_youtube_plain" if mode == "plain" else "c2_youtube_minibatch",
-                               sgns_form=mode, l2="flushed between steps (256 MB write)",
+                "config": dict(WORKLOAD, workload="c2_youtube_" + form,
+                               sgns_form=form, l2="flushed between steps (256 MB write)",
                                parallelism=f"replicas x{world}"),
                 "walk_steps_per_s": steps_ / (walk_ms / 1e3), "sgns_words_per_s": words / (train_ms / 1e3),
                 "walk_ms_per_step": walk_ms / args.steps, "sgns_ms_per_step": train_ms / args.steps,
@@ -393,13 +401,13 @@ def run_auc_ours(args, local):
         clocks = Clocks(local)
         clocks.start()
         res = embed(graph, mode=mode, seed=args.seed, workers=workers, deterministic=2 if variant == "adjoint" else 0,
-                    device=local, **AUC_HP)
+                    master_rows=args.master_rows, device=local, **AUC_HP)
         clk = clocks.stop()
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
                           "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16",
-                          "workers": workers or res["workers"], "auc": m["auc"],
+                          "workers": workers or res["workers"], "master_rows": args.master_rows, "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
                           "walk_steps_per_s": res["walk_steps_per_s"], "sgns_words_per_s": res["words_per_s"],
@@ -466,9 +474,10 @@ def run_profile_case(args, local):
     p2 = eng.run_round(v_num, 3, n_walkers=args.profile_walks)
     out = {"case": args.profile, "walks": args.profile_walks, "walk_ms": p2.info.walk_ms,
            "draws": p2.info.draws, "footprints": p2.info.footprints}
-    if args.profile in ("sgns", "minibatch"):
-        s = SGNS(v_num, counts, size=128, window=10, negative=5, sample=1e-3, alpha=0.01, iter=1, min_count=0,
-                 mode="plain" if args.profile == "sgns" else "minibatch", seed=1, device=local)
+    if args.profile in ("sgns", "minibatch", "adjoint"):
+        s = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
+                 min_count=0, mode="minibatch" if args.profile == "minibatch" else "plain", seed=1,
+                 deterministic=2 if args.profile == "adjoint" else 0, device=local)
         info = s.train_paths(p2)
         out.update({"train_ms": info.train_ms, "pairs": info.pairs, "words": info.words})
         s.close()
@@ -479,7 +488,7 @@ def run_profile_case(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["walk", "sgns", "minibatch"], default=None,
+    ap.add_argument("--profile", choices=["walk", "sgns", "minibatch", "adjoint"], default=None,
                     help="run one small launch of a kernel for ncu and exit")
     ap.add_argument("--profile-walks", type=int, default=50_000)
     ap.add_argument("--gpus", type=int, default=1)
@@ -488,6 +497,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["plain", "minibatch"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
     ap.add_argument("--auc", action="store_true",
                     help="run the whole embedding job on a 10%%-held-out split and print link-prediction AUC lines")
@@ -496,6 +506,7 @@ def main():
     ap.add_argument("--auc-modes", default="plain,minibatch")
     ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
     ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--master-rows", type=int, default=0, help="--auc: FP32 master rows of the minibatch form")
     ap.add_argument("--tmpdir", default=None)
     ap.add_argument("--ref-timeout", type=int, default=7200)
     args = ap.parse_args()

@@ -111,18 +111,32 @@ __global__ void __launch_bounds__(kAdjThreads) sgns_adjoint_kernel(AdjArgs a) {
             }
         }
         double loss = 0.0;
+        // Consecutive pairs usually share their output row (the contexts of one
+        // centre): its row stays in registers and its gradient is summed in
+        // order over the run, then added to the accumulator once.
+        uint32_t run_o = 0xFFFFFFFFu;
+        float uo[V], duo[V];
         for (uint64_t p = p0; p < p1; p++) {
             const uint32_t i = a.inputs[p], o = a.outputs[p];
-            float v[V], uo[V], dv[V], duo[V];
+            if (o != run_o) {
+                if (run_o != 0xFFFFFFFFu) {
+#pragma unroll
+                    for (int c = 0; c < V; c++) fix_add(a.acc_out + (size_t)run_o * D + col + c, duo[c], a.flag);
+                }
+                adj_load<V>(a.out_f32, a.out_bf, a.out_master, a.n_master, o, col, uo);
+#pragma unroll
+                for (int c = 0; c < V; c++) duo[c] = 0.f;
+                run_o = o;
+            }
+            float v[V], dv[V];
             adj_load<V>(a.in_f32, a.in_bf, a.in_master, a.n_master, i, col, v);
-            adj_load<V>(a.out_f32, a.out_bf, a.out_master, a.n_master, o, col, uo);
             const float s = adj_dot<V>(v, uo);
             const float g = -1.f / (1.f + expf(s));   // sigmoid(s) - 1
             if (a.batch_loss) loss += softplus(-(double)s);
 #pragma unroll
             for (int c = 0; c < V; c++) {
                 dv[c] = __fmul_rn(g, uo[c]);
-                duo[c] = __fmul_rn(g, v[c]);
+                duo[c] = fmaf(g, v[c], duo[c]);
             }
             for (int k = 0; k < neg; k++) {
                 float u[V];
@@ -138,10 +152,11 @@ __global__ void __launch_bounds__(kAdjThreads) sgns_adjoint_kernel(AdjArgs a) {
                 }
             }
 #pragma unroll
-            for (int c = 0; c < V; c++) {
-                fix_add(a.acc_in + (size_t)i * D + col + c, dv[c], a.flag);
-                fix_add(a.acc_out + (size_t)o * D + col + c, duo[c], a.flag);
-            }
+            for (int c = 0; c < V; c++) fix_add(a.acc_in + (size_t)i * D + col + c, dv[c], a.flag);
+        }
+        if (run_o != 0xFFFFFFFFu) {
+#pragma unroll
+            for (int c = 0; c < V; c++) fix_add(a.acc_out + (size_t)run_o * D + col + c, duo[c], a.flag);
         }
         for (int k = 0; k < neg; k++) {
             const uint32_t w = a.negatives[b * neg + k];

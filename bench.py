@@ -243,6 +243,19 @@ def run_ours(args, rank, world, local, pg):
     wp = _lib.WalkParams(min_len=20, init_round=10, walker_num=v_num, max_len=64, seed=2024 + rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
 
+    # Launch shapes timed on this workload before anything is measured (dg_walk_autotune, dg_sgns_autotune).
+    tune = {}
+    if not args.no_autotune:
+        ti = _lib.TuneInfo()
+        check(L.dg_walk_autotune(graph.handle, C.byref(wp), 2, v_num, C.byref(ti)))
+        tune["walk"] = ti.as_dict()
+        ph = C.c_void_p()
+        check(L.dg_walk_run_round(graph.handle, C.byref(wp), 90, v_num, C.byref(ph)))
+        ti = _lib.TuneInfo()
+        check(L.dg_sgns_autotune(sgns.handle, ph, C.byref(ti)))
+        tune["sgns"] = ti.as_dict()
+        L.dg_paths_free(ph)
+
     def step(r):
         info = _lib.PipelineInfo()
         check(L.dg_pipeline_round(graph.handle, sgns.handle, C.byref(wp), r, v_num, C.c_float(0.0),
@@ -364,7 +377,8 @@ def run_ours(args, rank, world, local, pg):
                 "footprints_per_step": fp / args.steps, "pairs_per_step": pairs / args.steps,
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
                         "d2h_bytes_per_step": d2h / args.steps},
-                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu}
+                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
+                "autotune": tune}
     sgns.close()
     graph.close()
     return line
@@ -497,6 +511,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["plain", "minibatch"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
     ap.add_argument("--auc", action="store_true",

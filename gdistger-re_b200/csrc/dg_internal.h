@@ -115,6 +115,7 @@ struct dg_graph {
     std::vector<double> entropy_history;
     uint64_t visits_total = 0;        // footprints over all rounds (sum of freq)
     double threshold_ms = 0.0;
+    int walk_shape = 0;               // walk_kernel launch shape (dg_walk_autotune)
     ~dg_graph();
 };
 

@@ -251,9 +251,9 @@ __device__ __forceinline__ int32_t negative_target(const SgnsArgs &a, uint32_t p
 // Handles negative <= kFastNeg; larger counts use sgns_plain_seq_kernel.
 constexpr int kFastNeg = 8;
 
-template <int VEC>
-__global__ void __launch_bounds__(kPlainThreads) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
-    __shared__ int32_t sen_all[kPlainThreads / 32][kMaxSentence];
+template <int VEC, int THREADS>
+__global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
     int32_t *sen = sen_all[warp];
@@ -557,6 +557,44 @@ int adjoint_pairs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
     return DG_OK;
 }
 
+// An explicit worker count (warps) lowers the resident grid, never raises it.
+static int plain_blocks(const dg_sgns *s, int resident, int threads) {
+    if (s->p.workers == 0) return resident;
+    const int want = (int)((s->p.workers + threads / 32 - 1) / (threads / 32));
+    return std::max(1, std::min(resident, want));
+}
+
+// One launch of the fast plain kernel in launch shape I (threads per block,
+// blocks per SM); dg_sgns_autotune picks the shape.
+template <int V, int I>
+static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    constexpr int T = kPlainShapes[I].threads;
+    int blocks = 1, threads = 32;
+    if (!s->p.deterministic) {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sgns_plain_kernel<V, T>, T, 0);
+        per_sm = std::max(per_sm, 1);
+        if (kPlainShapes[I].per_sm > 0) per_sm = std::min(per_sm, kPlainShapes[I].per_sm);
+        blocks = plain_blocks(s, dg::sm_count(s->device) * per_sm, T);
+        threads = T;
+    }
+    sgns_plain_kernel<V, T><<<blocks, threads, 0, s->stream>>>(a, ws);
+}
+
+template <int V>
+static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    static_assert(kPlainShapeCount == 5, "dispatch below lists every shape");
+    switch (s->plain_shape) {
+    case 0: plain_fast_launch<V, 0>(s, a, ws); break;
+    case 1: plain_fast_launch<V, 1>(s, a, ws); break;
+    case 2: plain_fast_launch<V, 2>(s, a, ws); break;
+    case 3: plain_fast_launch<V, 3>(s, a, ws); break;
+    case 4: plain_fast_launch<V, 4>(s, a, ws); break;
+    default: return dg::fail(DG_ERR_ARG, "plain launch shape %d out of range", s->plain_shape);
+    }
+    return DG_OK;
+}
+
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     const int vec = s->p.size / 32;
     int blocks = 1, threads = 32;
@@ -566,21 +604,16 @@ int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
         return std::max(per_sm, 1);
     };
     if (!s->p.deterministic) threads = kPlainThreads;
-    // An explicit worker count (warps) lowers the resident grid, never raises it.
-    auto cap = [&](int resident) {
-        if (s->p.workers == 0) return resident;
-        const int want = (int)((s->p.workers + kPlainThreads / 32 - 1) / (kPlainThreads / 32));
-        return std::max(1, std::min(resident, want));
-    };
     const bool fast = a.negative <= kFastNeg;
     switch (vec) {
 #define DG_PLAIN_CASE(V)                                                                             \
     case V:                                                                                          \
         if (fast) {                                                                                  \
-            if (!s->p.deterministic) blocks = cap(dg::sm_count(s->device) * occ(sgns_plain_kernel<V>)); \
-            sgns_plain_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                          \
+            int rc_ = plain_fast_shape<V>(s, a, ws);                                                 \
+            if (rc_) return rc_;                                                                     \
         } else {                                                                                     \
-            if (!s->p.deterministic) blocks = cap(dg::sm_count(s->device) * occ(sgns_plain_seq_kernel<V>)); \
+            if (!s->p.deterministic)                                                                 \
+                blocks = plain_blocks(s, dg::sm_count(s->device) * occ(sgns_plain_seq_kernel<V>), kPlainThreads); \
             sgns_plain_seq_kernel<V><<<blocks, threads, 0, s->stream>>>(a, ws);                      \
         }                                                                                            \
         dg::note_launch();                                                                           \
@@ -776,6 +809,81 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
         info->pairs = st[2];
         info->train_ms = t.ms();
     }
+    return DG_OK;
+}
+
+extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alpha, dg_train_info *info);
+
+// Times every launch shape of the plain kernel on these walks and keeps the
+// fastest.  Rows and the pass counter are restored after each trial, so tuning
+// leaves the trainer as it found it (apart from the launch shape).  Only the
+// plain form's Hogwild kernel has shapes to choose from; other configurations
+// report one candidate.
+extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info *info) {
+    DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_autotune: NULL argument");
+    dg_tune_info r{};
+    if (s->p.mode != DG_SGNS_PLAIN || s->p.deterministic || s->p.negative > dgs::kFastNeg) {
+        r.n_candidates = 1;
+        r.chosen = 0;
+        if (info) *info = r;
+        return DG_OK;
+    }
+    dg::DeviceGuard guard(s->device);
+    const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
+    dg::DevArray<float> s0, s1;
+    DG_CUDA(s0.alloc(n));
+    DG_CUDA(s1.alloc(n));
+    DG_CUDA(cudaMemcpyAsync(s0.p, s->syn0.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+    DG_CUDA(cudaMemcpyAsync(s1.p, s->syn1.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+    const uint32_t pass0 = s->pass;
+    const int shape0 = s->plain_shape;
+    auto restore = [&]() -> int {
+        DG_CUDA(cudaMemcpyAsync(s->syn0.p, s0.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+        DG_CUDA(cudaMemcpyAsync(s->syn1.p, s1.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+        DG_CUDA(cudaStreamSynchronize(s->stream));
+        s->pass = pass0;
+        return DG_OK;
+    };
+    r.n_candidates = dgs::kPlainShapeCount;
+    double best = 1e300;
+    for (int k = 0; k < dgs::kPlainShapeCount; k++) {
+        s->plain_shape = k;
+        double ms = 0.0;
+        for (int rep = 0; rep < 2; rep++) {   // the first run warms caches
+            int rc = restore();
+            if (!rc) {
+                dg_train_info ti{};
+                rc = dg_sgns_train_paths(s, paths, 0.0f, &ti);
+                ms = ti.train_ms;
+            }
+            if (rc) {
+                s->plain_shape = shape0;
+                restore();
+                return rc;
+            }
+        }
+        if (k < DG_TUNE_MAX) {
+            r.ms[k] = ms;
+            r.shape[k][0] = dgs::kPlainShapes[k].threads;
+            r.shape[k][1] = dgs::kPlainShapes[k].per_sm;
+        }
+        if (ms < best) {
+            best = ms;
+            r.chosen = k;
+        }
+    }
+    int rc = restore();
+    if (rc) return rc;
+    s->plain_shape = r.chosen;
+    if (info) *info = r;
+    return DG_OK;
+}
+
+extern "C" int dg_sgns_set_shape(dg_sgns *s, int shape) {
+    DG_CHECK(s, DG_ERR_ARG, "dg_sgns_set_shape: NULL trainer");
+    DG_CHECK(shape >= 0 && shape < dgs::kPlainShapeCount, DG_ERR_ARG, "plain launch shape %d out of range [0, %d)",
+             shape, dgs::kPlainShapeCount);
+    s->plain_shape = shape;
     return DG_OK;
 }
 

@@ -16,6 +16,13 @@ constexpr int kMaxExp = 6;                        // word2vec.cu:30
 constexpr uint64_t kDefaultTableSize = 100000000; // word2vec.cu:66
 constexpr uint32_t kMaxSentence = 1024;           // tokens of one walk used for training
 constexpr int kPlainThreads = 256;
+// Launch shapes of the fast plain kernel: threads per block (one walk per warp)
+// and blocks per SM (0: as many as fit).  Shape 0 is the default.
+struct PlainShape {
+    int threads, per_sm;
+};
+constexpr PlainShape kPlainShapes[] = {{256, 0}, {128, 0}, {64, 0}, {256, 2}, {128, 4}};
+constexpr int kPlainShapeCount = (int)(sizeof(kPlainShapes) / sizeof(kPlainShapes[0]));
 constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
 
 // Philox counter word 3 of each random choice (counter words 0-2: index, walk, pass).
@@ -93,6 +100,7 @@ struct dg_sgns {
     uint32_t vocab_size = 0;
     uint32_t n_master = 0;
     uint32_t mb_workers = 0;           // minibatch form: staleness bound on concurrent workers
+    int plain_shape = 0;               // plain form: launch shape (dg_sgns_autotune)
     uint64_t train_words = 0;
     uint32_t pass = 0;
     std::vector<uint32_t> vocab_ids, vocab_cn;

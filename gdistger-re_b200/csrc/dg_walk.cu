@@ -14,8 +14,14 @@
 
 namespace {
 
-constexpr int kWalkThreads = 256;
-constexpr int kSmemSteps = 24;           // footprints cached per thread in shared memory
+// Launch shapes of walk_kernel: walks per block (one walk per thread) and the
+// first footprints of each walk cached in shared memory.  Variant 0 is the
+// default; dg_walk_autotune times them all and keeps the fastest per graph.
+struct WalkShape {
+    int threads, steps;
+};
+constexpr WalkShape kWalkShapes[] = {{256, 24}, {128, 24}, {256, 16}, {256, 32}, {512, 16}, {128, 48}};
+constexpr int kWalkShapeCount = (int)(sizeof(kWalkShapes) / sizeof(kWalkShapes[0]));
 constexpr uint32_t kWalkTag = 0x57414C4Bu; // Philox counter word 3 for walk draws ("WALK")
 constexpr uint32_t kDefaultStride = 64;
 
@@ -76,8 +82,9 @@ __device__ __forceinline__ unsigned long long warp_sum(unsigned long long v) {
 // integer compare.  The walk's footprints go to its arena slot and, for the first
 // kSmemSteps, to a shared-memory copy that serves the prior-visit count
 // (the unordered_map of walk.hpp:816).
-__global__ void __launch_bounds__(kWalkThreads) walk_kernel(WalkArgs a) {
-    __shared__ uint32_t cache[kSmemSteps][kWalkThreads];
+template <int THREADS, int STEPS>
+__global__ void __launch_bounds__(THREADS) walk_kernel(WalkArgs a) {
+    __shared__ uint32_t cache[STEPS][THREADS];
     const int tid = threadIdx.x;
     unsigned long long n_fp = 0, n_draw = 0, n_trace = 0, n_over = 0;
     uint32_t longest = 0;
@@ -91,13 +98,13 @@ __global__ void __launch_bounds__(kWalkThreads) walk_kernel(WalkArgs a) {
         // Appends v and returns its prior-visit count.
         auto visit_count = [&](uint32_t v) -> uint32_t {
             uint32_t c = 0;
-            const uint32_t hot = n < (uint32_t)kSmemSteps ? n : (uint32_t)kSmemSteps;
+            const uint32_t hot = n < (uint32_t)STEPS ? n : (uint32_t)STEPS;
             for (uint32_t i = 0; i < hot; i++) c += cache[i][tid] == v;
-            for (uint32_t i = kSmemSteps; i < n; i++) c += path[i] == v;
+            for (uint32_t i = STEPS; i < n; i++) c += path[i] == v;
             return c;
         };
         auto push = [&](uint32_t v) {
-            if (n < (uint32_t)kSmemSteps) cache[n][tid] = v;
+            if (n < (uint32_t)STEPS) cache[n][tid] = v;
             path[n] = v;
             atomicAdd(&a.freq[v], 1u);
             n++;
@@ -240,8 +247,39 @@ int relative_entropy(dg_graph *g, uint64_t words_sum, double *h) {
     return DG_OK;
 }
 
+// One launch of walk_kernel in launch shape I: a persistent grid of as many
+// blocks as fit (each thread pulls walker ids from the queue).
+template <int I>
+int walk_launch_shape(dg_graph *g, const WalkArgs &a, uint32_t n_walkers) {
+    constexpr int T = kWalkShapes[I].threads, S = kWalkShapes[I].steps;
+    int per_sm = 0;
+    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel<T, S>, T, 0));
+    if (per_sm < 1) per_sm = 1;
+    uint64_t blocks = (uint64_t)dg::sm_count(g->device) * per_sm;
+    const uint64_t needed = ((uint64_t)n_walkers + T - 1) / T;
+    if (blocks > needed) blocks = needed ? needed : 1;
+    walk_kernel<T, S><<<(unsigned)blocks, T, 0, g->stream>>>(a);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
+int walk_launch(int shape, dg_graph *g, const WalkArgs &a, uint32_t n_walkers) {
+    static_assert(kWalkShapeCount == 6, "dispatch below lists every shape");
+    switch (shape) {
+    case 0: return walk_launch_shape<0>(g, a, n_walkers);
+    case 1: return walk_launch_shape<1>(g, a, n_walkers);
+    case 2: return walk_launch_shape<2>(g, a, n_walkers);
+    case 3: return walk_launch_shape<3>(g, a, n_walkers);
+    case 4: return walk_launch_shape<4>(g, a, n_walkers);
+    case 5: return walk_launch_shape<5>(g, a, n_walkers);
+    default: return dg::fail(DG_ERR_ARG, "walk launch shape %d out of range", shape);
+    }
+}
+
+// shape < 0: the graph's current (tuned) launch shape.
 int run_round(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_walkers, uint32_t stride,
-              std::unique_ptr<dg_paths> &out) {
+              std::unique_ptr<dg_paths> &out, int shape = -1) {
     DG_CHECK(stride >= 2 && stride <= (1u << 16), DG_ERR_ARG, "max_len %u out of range [2, 65536]", stride);
     int rc = dg::ensure_entropy_table(g, stride);
     if (rc) return rc;
@@ -283,17 +321,10 @@ int run_round(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_w
     a.seed_lo = (uint32_t)p->seed;
     a.seed_hi = (uint32_t)(p->seed >> 32);
 
-    int per_sm = 0;
-    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, walk_kernel, kWalkThreads, 0));
-    if (per_sm < 1) per_sm = 1;
-    uint64_t blocks = (uint64_t)dg::sm_count(g->device) * per_sm;
-    const uint64_t needed = ((uint64_t)n_walkers + kWalkThreads - 1) / kWalkThreads;
-    if (blocks > needed) blocks = needed ? needed : 1;
-
     dg::EventTimer t;
     t.start(g->stream);
-    walk_kernel<<<(unsigned)blocks, kWalkThreads, 0, g->stream>>>(a); dg::note_launch();
-    DG_CUDA(cudaGetLastError());
+    rc = walk_launch(shape < 0 ? g->walk_shape : shape, g, a, n_walkers);
+    if (rc) return rc;
     t.stop(g->stream);
     unsigned long long h_stats[4];
     uint32_t h_ctl[2];
@@ -413,4 +444,59 @@ extern "C" void dg_paths_free(dg_paths *ps) {
     dg::DeviceGuard guard(ps->device);
     cudaStreamSynchronize(ps->g->stream);
     delete ps;
+}
+
+// Times every launch shape of walk_kernel on `n_walkers` walkers of `round` and
+// keeps the fastest for this graph.  Walks do not depend on the shape (each
+// walker's draws are keyed by its id), so tuning changes speed only; the visit
+// counts the trial rounds add are restored, and no round is recorded.
+extern "C" int dg_walk_autotune(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_walkers,
+                                dg_tune_info *info) {
+    DG_CHECK(g && p, DG_ERR_ARG, "dg_walk_autotune: NULL argument");
+    DG_CHECK(round > 0, DG_ERR_ARG, "dg_walk_autotune: rounds are numbered from 1");
+    uint64_t n = n_walkers ? n_walkers : p->walker_num;
+    DG_CHECK(n > 0 && n < (1ull << 32), DG_ERR_ARG, "walker count %llu out of range", (unsigned long long)n);
+    const uint32_t stride = p->max_len ? p->max_len : kDefaultStride;
+    dg::DeviceGuard guard(g->device);
+    dg::DevArray<uint32_t> saved;
+    DG_CUDA(saved.alloc(g->v_num));
+    DG_CUDA(cudaMemcpyAsync(saved.p, g->freq.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToDevice, g->stream));
+    dg_tune_info r{};
+    r.n_candidates = kWalkShapeCount;
+    double best = 1e300;
+    for (int k = 0; k < kWalkShapeCount; k++) {
+        double ms = 0.0;
+        for (int rep = 0; rep < 2; rep++) {   // the first run warms caches and the queue
+            std::unique_ptr<dg_paths> ps;
+            int rc = run_round(g, p, round, (uint32_t)n, stride, ps, k);
+            if (rc) {
+                cudaMemcpyAsync(g->freq.p, saved.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToDevice, g->stream);
+                cudaStreamSynchronize(g->stream);
+                return rc;
+            }
+            ms = ps->info.walk_ms;
+        }
+        if (k < DG_TUNE_MAX) {
+            r.ms[k] = ms;
+            r.shape[k][0] = kWalkShapes[k].threads;
+            r.shape[k][1] = kWalkShapes[k].steps;
+        }
+        if (ms < best) {
+            best = ms;
+            r.chosen = k;
+        }
+    }
+    DG_CUDA(cudaMemcpyAsync(g->freq.p, saved.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToDevice, g->stream));
+    DG_CUDA(cudaStreamSynchronize(g->stream));
+    g->walk_shape = r.chosen;
+    if (info) *info = r;
+    return DG_OK;
+}
+
+extern "C" int dg_walk_set_shape(dg_graph *g, int shape) {
+    DG_CHECK(g, DG_ERR_ARG, "dg_walk_set_shape: NULL graph");
+    DG_CHECK(shape >= 0 && shape < kWalkShapeCount, DG_ERR_ARG, "walk launch shape %d out of range [0, %d)", shape,
+             kWalkShapeCount);
+    g->walk_shape = shape;
+    return DG_OK;
 }

@@ -79,6 +79,17 @@ class SgnsPairs(C.Structure):
                 ("n_pairs", C.c_uint64), ("batch", C.c_uint32), ("negative", C.c_int)]
 
 
+class TuneInfo(C.Structure):
+    """dg_tune_info: the launch shapes timed by an autotune call and the one kept."""
+    _fields_ = [("n_candidates", C.c_int), ("chosen", C.c_int), ("shape", (C.c_int * 2) * 8),
+                ("ms", C.c_double * 8)]
+
+    def as_dict(self) -> dict:
+        n = min(self.n_candidates, 8)
+        return {"chosen": self.chosen, "candidates": [{"shape": [self.shape[k][0], self.shape[k][1]],
+                                                       "ms": self.ms[k]} for k in range(n)]}
+
+
 _P = C.c_void_p
 _SIGS = {
     "dg_last_error": ([], C.c_char_p),
@@ -110,6 +121,10 @@ _SIGS = {
     "dg_sgns_minibatch_train_noalloc": ([C.POINTER(MinibatchArgs), _P, C.POINTER(TrainInfo)], C.c_int),
     "dg_sgns_loss_grad": ([_P, C.POINTER(SgnsPairs), C.POINTER(C.c_double), _P, _P], C.c_int),
     "dg_sgns_adjoint_step": ([_P, C.POINTER(SgnsPairs), C.c_float, C.POINTER(C.c_double)], C.c_int),
+    "dg_walk_autotune": ([_P, C.POINTER(WalkParams), C.c_uint32, C.c_uint32, C.POINTER(TuneInfo)], C.c_int),
+    "dg_walk_set_shape": ([_P, C.c_int], C.c_int),
+    "dg_sgns_autotune": ([_P, _P, C.POINTER(TuneInfo)], C.c_int),
+    "dg_sgns_set_shape": ([_P, C.c_int], C.c_int),
 }
 
 _lib = None

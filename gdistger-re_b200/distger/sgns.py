@@ -51,6 +51,13 @@ class SGNS:
     def handle(self):
         return self._h
 
+    def autotune(self, paths) -> dict:
+        """Times the plain kernel's launch shapes on these walks and keeps the fastest
+        (rows and pass counter restored)."""
+        info = _lib.TuneInfo()
+        check(lib().dg_sgns_autotune(self._h, paths.handle, C.byref(info)))
+        return info.as_dict()
+
     def train_paths(self, paths, alpha: float = 0.0) -> _lib.TrainInfo:
         info = _lib.TrainInfo()
         check(lib().dg_sgns_train_paths(self._h, paths.handle, alpha, C.byref(info)))

@@ -158,6 +158,16 @@ class WalkEngine:
         return _lib.WalkParams(min_len=self.minLength, init_round=self.init_round, walker_num=walker_num,
                                max_len=self.max_len, seed=self.seed)
 
+    def autotune(self, walker_num: int, round_index: int = 2, n_walkers: int = 0) -> dict:
+        """Times the walk kernel's launch shapes on this graph and keeps the fastest
+        (walks are identical under every shape; visit counts are rolled back)."""
+        if self.graph is None:
+            raise RuntimeError("load_graph first")
+        info = _lib.TuneInfo()
+        check(lib().dg_walk_autotune(self.graph.handle, C.byref(self.params(walker_num)), round_index, n_walkers,
+                                     C.byref(info)))
+        return info.as_dict()
+
     def run_round(self, walker_num: int, round_index: int, n_walkers: int = 0) -> Paths:
         if self.graph is None:
             raise RuntimeError("load_graph first")

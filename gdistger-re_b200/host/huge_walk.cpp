@@ -25,8 +25,10 @@
 //   -rounds n               stop after round n (default 30)
 //   -train-from n           first round whose walks are trained (default 1;
 //                           word2vec.cu:1286 starts at round 3)
-//   -seed s  -device d  -deterministic 0|1  -master-rows n  -table-size n  -max-len n
+//   -seed s  -device d  -master-rows n  -table-size n  -max-len n
+//   -deterministic 0|1|2    0 Hogwild, 1 one worker in order, 2 adjoint gradient steps
 //   -workers n              concurrent trainer workers (0 = automatic)
+//   -autotune 0|1           time the kernels' launch shapes first (default 1)
 #include <chrono>
 #include <cmath>
 #include <cstdint>
@@ -52,6 +54,7 @@ struct Options {
     int rounds = 30, train_from = 1, device = 0, deterministic = 0, max_len = 0;
     uint64_t seed = 1;
     uint32_t master_rows = 0, workers = 0;
+    int autotune = 1;
     uint64_t table_size = 0;
 };
 
@@ -112,6 +115,7 @@ Options parse(int argc, char **argv) {
         else if (a == "-table-size") o.table_size = strtoull(val(), nullptr, 10);
         else if (a == "-max-len") o.max_len = i32();
         else if (a == "-workers") o.workers = u32();
+        else if (a == "-autotune") o.autotune = i32();
         else die(("unknown flag " + a).c_str());
     }
     // option_helper.hpp asserts -v, -g, --min_L, --min_R and -w are present.
@@ -188,13 +192,47 @@ int main(int argc, char **argv) {
     wp.seed = o.seed;
 
     auto lr = make_lr(o);
+    if (o.autotune) {
+        // Launch shapes timed on this graph; walks do not depend on them and the
+        // trial rounds' visit counts are rolled back.
+        dg_tune_info ti{};
+        check(dg_walk_autotune(g, &wp, 2, 0, &ti), "dg_walk_autotune");
+        printf("autotune walk_kernel: shape %d of %d (%d walks per block, %d cached steps)\n", ti.chosen,
+               ti.n_candidates, ti.shape[ti.chosen][0], ti.shape[ti.chosen][1]);
+    }
     const auto t_embed = std::chrono::steady_clock::now();
     double walk_ms = 0, train_ms = 0, device_ms = 0;
     uint64_t steps = 0, footprints = 0, words = 0, pairs = 0;
     for (int r = 1; r <= o.rounds; r++) {
         dg_paths *keep = nullptr;
         dg_paths **keep_arg = o.walk_prefix.empty() ? nullptr : &keep;
-        if (r >= o.train_from) {
+        if (r >= o.train_from && o.autotune && r == o.train_from) {
+            // The first trained round's walks also time the trainer's launch
+            // shapes (rows are restored after every trial), then train.
+            const float alpha = lr->get_lr();
+            dg_paths *p = nullptr;
+            check(dg_walk_run_round(g, &wp, static_cast<uint32_t>(r), 0, &p), "dg_walk_run_round");
+            dg_tune_info ti{};
+            check(dg_sgns_autotune(s, p, &ti), "dg_sgns_autotune");
+            if (ti.n_candidates > 1)
+                printf("autotune SGNS: shape %d of %d (%d threads per block, %d blocks per SM)\n", ti.chosen,
+                       ti.n_candidates, ti.shape[ti.chosen][0], ti.shape[ti.chosen][1]);
+            dg_round_info ri{};
+            check(dg_paths_get_info(p, &ri), "dg_paths_get_info");
+            dg_train_info tr{};
+            check(dg_sgns_train_paths(s, p, alpha, &tr), "dg_sgns_train_paths");
+            walk_ms += ri.walk_ms;
+            train_ms += tr.train_ms;
+            device_ms += ri.walk_ms + tr.train_ms;
+            steps += ri.steps;
+            footprints += ri.footprints;
+            words += tr.words;
+            pairs += tr.pairs;
+            printf("round %d: walks %u steps %llu Delat RE %g alpha %.9g walk %.3f ms train %.3f ms (%llu words)\n", r,
+                   ri.n_walks, static_cast<unsigned long long>(ri.steps), std::fabs(ri.delta_h), alpha, ri.walk_ms,
+                   tr.train_ms, static_cast<unsigned long long>(tr.words));
+            if (keep_arg) keep = p; else dg_paths_free(p);
+        } else if (r >= o.train_from) {
             const float alpha = lr->get_lr();
             dg_pipeline_info pi{};
             check(dg_pipeline_round(g, s, &wp, static_cast<uint32_t>(r), 0, alpha, &pi, keep_arg), "dg_pipeline_round");

@@ -209,6 +209,35 @@ DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *ou
  * (word2vec.cu:1353-1362). */
 DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
 
+/* -------------------------------------------------------------- autotuner */
+
+/* No counterpart in the reference (its kernels have fixed launches).  Each
+ * kernel with a choice of launch shapes is timed on live data, every shape
+ * twice (the second run is kept), and the fastest shape is kept by the handle
+ * for later calls.  Results never depend on the shape: walks are keyed by
+ * walker id, and the plain trainer's Hogwild updates depend on scheduling
+ * under every shape alike. */
+#define DG_TUNE_MAX 8
+typedef struct {
+    int n_candidates;
+    int chosen;                /* index of the shape kept */
+    int shape[DG_TUNE_MAX][2]; /* walks: {walks per block, footprints cached in shared memory per walk};
+                                  plain SGNS: {threads per block, blocks per SM (0 = as many as fit)} */
+    double ms[DG_TUNE_MAX];    /* kernel time of each candidate (CUDA events) */
+} dg_tune_info;
+
+/* Times walk_kernel's launch shapes on n_walkers (0: walker_num) walkers of
+ * `round`; the trial rounds' visit counts are rolled back and no round is
+ * recorded. */
+DG_API int dg_walk_autotune(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_walkers,
+                            dg_tune_info *info);
+DG_API int dg_walk_set_shape(dg_graph *g, int shape);
+
+/* Times the plain trainer's launch shapes on these walks; rows and the pass
+ * counter are restored after every trial. */
+DG_API int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info *info);
+DG_API int dg_sgns_set_shape(dg_sgns *s, int shape);
+
 /* ------------------------------------------------- SGNS loss and adjoint */
 
 /* Explicit minibatches for the loss / gradient entry points: n_pairs (input,

@@ -470,6 +470,62 @@ def run_auc_reference(args):
                                      walkers_per_round=v, min_L=20, min_R=5)}), flush=True)
 
 
+# Graphs generated, split and built on the device (dg_edges_chung_lu, dg_edges_split,
+# dg_graph_create_from_device_edges); scored by dg_lp_auc.
+SYNTH = {
+    "c5_twitter": dict(n=41_652_230, m=1_470_000_000, beta=1.9, max_degree=3_000_000.0, weighted=False,
+                       holdout=0.01, min_r=5),
+    "c2_youtube_device": dict(n=1_138_499, m=2_990_443, beta=2.1, max_degree=28_000.0, weighted=True,
+                              holdout=0.1, min_r=5),
+}
+
+
+def run_auc_synth(args, local):
+    """The whole job on a device-generated graph: generate, hold out, build the CSR,
+    walk + train --rounds rounds per form, score on the device.  One JSON line per form."""
+    import torch
+    from distger.embed import embed
+    from distger.synth import EdgeList
+    torch.cuda.set_device(local)
+    cfg = SYNTH[args.workload]
+    for form in args.auc_modes.split(","):
+        mode, _, variant = form.partition("-")
+        t0 = time.perf_counter()
+        e = EdgeList.chung_lu(cfg["n"], cfg["m"], cfg["beta"], seed=0, max_degree=cfg["max_degree"],
+                              weighted=cfg["weighted"], device=local)
+        t1 = time.perf_counter()
+        n_edges = e.n
+        pairs = e.split(cfg["holdout"], seed=2)
+        t2 = time.perf_counter()
+        graph = e.graph()
+        t3 = time.perf_counter()
+        e.close()
+        clocks = Clocks(local)
+        clocks.start()
+        res = embed(graph, mode=mode, seed=args.seed, rounds=args.rounds, init_round=cfg["min_r"], max_len=32,
+                    deterministic=2 if variant == "adjoint" else 0, keep_trainer=True, device=local, **AUC_HP)
+        clk = clocks.stop()
+        t4 = time.perf_counter()
+        sgns = res.pop("trainer")
+        m = pairs.auc(sgns)
+        t5 = time.perf_counter()
+        print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
+                          "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16", "workers": res["workers"],
+                          "auc": m["auc"], "auc_cosine": m["auc_cosine"], "test_pairs": pairs.n_pos + pairs.n_neg,
+                          "vertices": cfg["n"], "undirected_edges": n_edges, "rounds": len(res["rounds"]),
+                          "generate_s": t1 - t0, "split_s": t2 - t1, "csr_build_s": t3 - t2,
+                          "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["wall_s"],
+                          "score_s": t5 - t4, "end_to_end_s": t5 - t0,
+                          "walk_steps_per_s": res["walk_steps_per_s"], "sgns_words_per_s": res["words_per_s"],
+                          "footprints": res["footprints"], "words": res["words"], "clocks": clk,
+                          "config": dict(AUC_HP, graph=dict(cfg), split_seed=2, walkers_per_round=cfg["n"],
+                                         min_L=20, lr="ExponentialDecayLR(alpha, 0.1)",
+                                         note="rounds 1..%d of 30" % args.rounds)}), flush=True)
+        sgns.close()
+        pairs.close()
+        graph.close()
+
+
 def run_profile_case(args, local):
     """A small case of one kernel for ncu: the YouTube-shaped graph and trainer
     (rows larger than L2), one walk round of --profile-walks walkers, then one
@@ -516,8 +572,10 @@ def main():
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
     ap.add_argument("--auc", action="store_true",
                     help="run the whole embedding job on a 10%%-held-out split and print link-prediction AUC lines")
-    ap.add_argument("--workload", choices=["c1_small", "c2_youtube", "c3_livejournal"], default="c1_small",
-                    help="graph of the --auc run")
+    ap.add_argument("--workload", choices=["c1_small", "c2_youtube", "c3_livejournal", "c5_twitter",
+                                           "c2_youtube_device"], default="c1_small",
+                    help="graph of the --auc run (c5_twitter and *_device: generated and split on the device)")
+    ap.add_argument("--rounds", type=int, default=30, help="--auc on device-generated graphs: walk rounds")
     ap.add_argument("--auc-modes", default="plain,minibatch")
     ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
     ap.add_argument("--seed", type=int, default=1)
@@ -531,6 +589,8 @@ def main():
     if args.auc:
         if args.impl == "reference":
             run_auc_reference(args)
+        elif args.workload in SYNTH:
+            run_auc_synth(args, int(os.environ.get("LOCAL_RANK", "0")))
         else:
             run_auc_ours(args, int(os.environ.get("LOCAL_RANK", "0")))
         return

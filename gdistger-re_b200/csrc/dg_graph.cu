@@ -2,6 +2,8 @@
 // thresholds, plus the entropy-term table the walk kernel reads.
 #include "dg_internal.h"
 
+#include <cub/cub.cuh>
+
 #include <cerrno>
 #include <climits>
 #include <cmath>
@@ -196,6 +198,112 @@ extern "C" int dg_graph_create_from_edges(const void *edges, uint64_t n_edges, u
                                           int device, dg_graph **out) {
     DG_CHECK(edges != nullptr || n_edges == 0, DG_ERR_ARG, "dg_graph_create_from_edges: edges is NULL");
     return build_graph(static_cast<const HostEdge *>(edges), n_edges, v_num, undirected, device, out);
+}
+
+// ------------------------------------------------- CSR from device edges
+
+namespace {
+
+__global__ void double_keys(const uint64_t *keys, uint64_t n, uint64_t *out) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = keys[i];
+        out[2 * i] = k;
+        out[2 * i + 1] = (k << 32) | (k >> 32);
+    }
+}
+
+// Row offsets of sorted directed keys (src in the high word), then the
+// neighbour and edge-data columns.
+__global__ void csr_columns(const uint64_t *d, uint64_t m, uint32_t v_num, uint64_t data_seed, int weighted,
+                            uint64_t *offsets, uint32_t *nbr, float *data) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t src = (uint32_t)(d[i] >> 32), dst = (uint32_t)d[i];
+        const int64_t prev = i == 0 ? -1 : (int64_t)(d[i - 1] >> 32);
+        for (int64_t v = prev + 1; v <= (int64_t)src; v++) offsets[v] = i;
+        if (i == m - 1)
+            for (uint64_t v = (uint64_t)src + 1; v <= v_num; v++) offsets[v] = m;
+        nbr[i] = dst;
+        const uint64_t key = src < dst ? ((uint64_t)src << 32) | dst : ((uint64_t)dst << 32) | src;
+        data[i] = dg::edge_data(key, data_seed, weighted);
+    }
+}
+
+__global__ void row_degrees(const uint64_t *offsets, uint32_t v_num, uint32_t *deg) {
+    for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < v_num; v += gridDim.x * blockDim.x)
+        deg[v] = (uint32_t)(offsets[v + 1] - offsets[v]);
+}
+
+}  // namespace
+
+// The undirected CSR of a device edge list (graph.hpp:671-686 doubling): every
+// pair contributes both directions, rows are sorted by neighbour, thresholds as
+// for a loaded graph.  Built entirely on the device.
+extern "C" int dg_graph_create_from_device_edges(const dg_edges *e, dg_graph **out) {
+    DG_CHECK(e && out, DG_ERR_ARG, "dg_graph_create_from_device_edges: NULL argument");
+    *out = nullptr;
+    const uint32_t v_num = e->v_num;
+    const uint64_t m = 2 * e->n;
+    dg::DeviceGuard guard(e->device);
+    std::unique_ptr<dg_graph> g(new dg_graph());
+    g->device = e->device;
+    g->v_num = v_num;
+    g->m = m;
+    DG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    cudaStream_t s = g->stream;
+    DG_CUDA(cudaStreamSynchronize(e->stream));
+    const unsigned grid = (unsigned)dg::sm_count(e->device) * 8;
+    DG_CUDA(g->offsets.alloc((size_t)v_num + 1));
+    DG_CUDA(g->out_deg.alloc(v_num));
+    DG_CUDA(g->in_deg.alloc(v_num));
+    DG_CUDA(g->freq.alloc(v_num));
+    DG_CUDA(cudaMemsetAsync(g->freq.p, 0, (size_t)v_num * 4, s));
+    if (m == 0) {
+        DG_CUDA(cudaMemsetAsync(g->offsets.p, 0, ((size_t)v_num + 1) * 8, s));
+        DG_CUDA(cudaMemsetAsync(g->out_deg.p, 0, (size_t)v_num * 4, s));
+        DG_CUDA(cudaMemsetAsync(g->in_deg.p, 0, (size_t)v_num * 4, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        *out = g.release();
+        return DG_OK;
+    }
+    dg::DevArray<uint64_t> d, alt;
+    DG_CUDA(d.alloc(m));
+    DG_CUDA(alt.alloc(m));
+    double_keys<<<grid, 256, 0, s>>>(e->keys.p, e->n, d.p);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    cub::DoubleBuffer<uint64_t> db(d.p, alt.p);
+    {
+        size_t bytes = 0;
+        DG_CUDA(cub::DeviceRadixSort::SortKeys(nullptr, bytes, db, m, 0, 64, s));
+        dg::DevArray<uint8_t> tmp;
+        DG_CUDA(tmp.alloc(bytes ? bytes : 1));
+        DG_CUDA(cub::DeviceRadixSort::SortKeys(tmp.p, bytes, db, m, 0, 64, s));
+    }
+    if (db.Current() != d.p) d.swap(alt);
+    alt.release();
+    dg::DevArray<uint32_t> nbr;
+    dg::DevArray<float> data;
+    DG_CUDA(nbr.alloc(m));
+    DG_CUDA(data.alloc(m));
+    csr_columns<<<grid, 256, 0, s>>>(d.p, m, v_num, e->data_seed, e->weighted, g->offsets.p, nbr.p, data.p);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaStreamSynchronize(s));
+    d.release();
+    row_degrees<<<grid, 256, 0, s>>>(g->offsets.p, v_num, g->out_deg.p);
+    dg::note_launch();
+    DG_CUDA(cudaMemcpyAsync(g->in_deg.p, g->out_deg.p, (size_t)v_num * 4, cudaMemcpyDeviceToDevice, s));
+    DG_CUDA(g->entries.alloc(m));
+    dg::EventTimer t;
+    t.start(s);
+    threshold_kernel<<<grid, 256, 0, s>>>(g->offsets.p, nbr.p, data.p, g->out_deg.p, v_num, g->entries.p);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    t.stop(s);
+    DG_CUDA(cudaStreamSynchronize(s));
+    g->threshold_ms = t.ms();
+    *out = g.release();
+    return DG_OK;
 }
 
 extern "C" int dg_graph_create(const char *edge_path, uint32_t v_num, int undirected, int device, dg_graph **out) {

@@ -49,6 +49,14 @@ struct DevArray {
         return cudaMalloc(reinterpret_cast<void **>(&p), count * sizeof(T));
     }
     size_t bytes() const { return n * sizeof(T); }
+    void swap(DevArray &o) {
+        T *tp = p;
+        p = o.p;
+        o.p = tp;
+        const size_t tn = n;
+        n = o.n;
+        o.n = tn;
+    }
 };
 
 // Sets the current device for the lifetime of the guard and restores the old one.
@@ -134,3 +142,41 @@ struct dg_paths {
 namespace dg {
 int ensure_entropy_table(dg_graph *g, uint32_t max_sn);
 }
+
+// Device-resident undirected edge list: unique keys (lo << 32 | hi), lo < hi, ascending.
+struct dg_edges {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    uint32_t v_num = 0;
+    uint64_t n = 0;
+    dg::DevArray<uint64_t> keys;
+    uint64_t data_seed = 0;
+    int weighted = 1;
+    ~dg_edges();
+};
+
+// Link-prediction test pairs on the device: positives first, then negatives.
+struct dg_lp_pairs {
+    int device = 0;
+    uint64_t n_pos = 0, n_neg = 0;
+    dg::DevArray<uint32_t> u, v;
+    dg::DevArray<uint8_t> label;
+    ~dg_lp_pairs();
+};
+
+namespace dg {
+// splitmix64 finaliser.
+__host__ __device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 30;
+    x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27;
+    x *= 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return x;
+}
+// Data of a generated undirected edge: uniform (0, 1] keyed by the pair, or 1.0.
+__host__ __device__ __forceinline__ float edge_data(uint64_t key, uint64_t seed, int weighted) {
+    if (!weighted) return 1.0f;
+    return 1.0f - (float)(mix64(key ^ seed) >> 40) * (1.0f / 16777216.0f);
+}
+}  // namespace dg

@@ -125,6 +125,16 @@ _SIGS = {
     "dg_walk_set_shape": ([_P, C.c_int], C.c_int),
     "dg_sgns_autotune": ([_P, _P, C.POINTER(TuneInfo)], C.c_int),
     "dg_sgns_set_shape": ([_P, C.c_int], C.c_int),
+    "dg_edges_chung_lu": ([_P, C.c_int, C.POINTER(_P)], C.c_int),
+    "dg_edges_get_info": ([_P, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)], C.c_int),
+    "dg_edges_copy": ([_P, _P, _P, _P], C.c_int),
+    "dg_edges_free": ([_P], None),
+    "dg_edges_split": ([_P, C.c_double, C.c_uint64, C.POINTER(_P)], C.c_int),
+    "dg_lp_pairs_get_info": ([_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)], C.c_int),
+    "dg_lp_pairs_copy": ([_P, _P, _P, _P], C.c_int),
+    "dg_lp_pairs_free": ([_P], None),
+    "dg_graph_create_from_device_edges": ([_P, C.POINTER(_P)], C.c_int),
+    "dg_lp_auc": ([_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
 }
 
 _lib = None

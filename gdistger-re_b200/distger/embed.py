@@ -37,18 +37,18 @@ def embed(graph: Graph, walker_num: int | None = None, mode: str = "plain", size
           negative: int = 5, batch_size: int = 21, sample: float = 1e-3, alpha: float = 0.01, iter: int = 1,
           min_count: int = 0, rounds: int = LAST_ROUND, init_round: int = 5, min_len: int = 20, lr: str = "exp",
           train_from: int = 1, seed: int = 1, master_rows: int = 0, workers: int = 0, deterministic: int = 0,
-          device: int = 0) -> dict:
+          max_len: int = 64, keep_trainer: bool = False, device: int = 0) -> dict:
     """Runs the job on `graph` and returns the embedding in vertex order plus the job's counters.
     deterministic = 2 trains by adjoint gradient steps (see dg_sgns_params)."""
     t0 = time.perf_counter()
     v_num = graph.v_num
     walker_num = walker_num or v_num
-    csr = graph.csr()
-    counts = csr["out_deg"] + csr["in_deg"]   # huge_walk.cpp:40-44
+    out_deg, in_deg = graph.degrees()
+    counts = out_deg + in_deg   # huge_walk.cpp:40-44
     sgns = SGNS(v_num, counts, size=size, window=window, negative=negative, batch_size=batch_size, sample=sample,
                 alpha=alpha, iter=iter, min_count=min_count, mode=mode, seed=seed, master_rows=master_rows,
                 workers=workers, deterministic=deterministic, device=device)
-    wp = _lib.WalkParams(min_len=min_len, init_round=init_round, walker_num=walker_num, max_len=64, seed=seed)
+    wp = _lib.WalkParams(min_len=min_len, init_round=init_round, walker_num=walker_num, max_len=max_len, seed=seed)
     sched = make_lr(lr, alpha, rounds)
     L = lib()
     acc = dict(walk_ms=0.0, train_ms=0.0, device_ms=0.0, steps=0, footprints=0, draws=0, words=0, pairs=0)
@@ -77,13 +77,17 @@ def embed(graph: Graph, walker_num: int | None = None, mode: str = "plain", size
         acc["footprints"] += w.footprints
         acc["draws"] += w.draws
         per_round.append({"round": r, "walks": w.n_walks, "steps": w.steps, "delta_h": abs(w.delta_h), "alpha": a})
-    rows, ids = sgns.embedding()
     t2 = time.perf_counter()
-    emb = np.zeros((v_num, size), np.float32)
-    emb[ids] = rows
     acc["workers"] = sgns.workers
-    sgns.close()
-    acc.update(rounds=per_round, embedding=emb, rounds_wall_s=t2 - t1, wall_s=t2 - t0,
+    if keep_trainer:
+        acc["trainer"] = sgns
+    else:
+        rows, ids = sgns.embedding()
+        emb = np.zeros((v_num, size), np.float32)
+        emb[ids] = rows
+        acc["embedding"] = emb
+        sgns.close()
+    acc.update(rounds=per_round, rounds_wall_s=t2 - t1, wall_s=t2 - t0,
                walk_steps_per_s=acc["steps"] / (acc["walk_ms"] * 1e-3) if acc["walk_ms"] else 0.0,
                words_per_s=acc["words"] / (acc["train_ms"] * 1e-3) if acc["train_ms"] else 0.0)
     return acc

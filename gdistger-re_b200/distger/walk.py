@@ -27,9 +27,11 @@ class Graph:
     """Device CSR (GraphEngine::load_graph, graph.hpp:642-824)."""
 
     def __init__(self, v_num: int, graph_path: str | None = None, edges: np.ndarray | None = None,
-                 make_undirected: bool = False, device: int = 0):
+                 make_undirected: bool = False, device: int = 0, handle=None):
         h = C.c_void_p()
-        if edges is not None:
+        if handle is not None:
+            h = handle
+        elif edges is not None:
             edges = np.ascontiguousarray(edges, dtype=EDGE_DTYPE)
             check(lib().dg_graph_create_from_edges(edges.ctypes.data if edges.size else None, edges.size,
                                                    v_num, int(make_undirected), device, C.byref(h)))
@@ -59,6 +61,13 @@ class Graph:
         check(lib().dg_graph_copy_csr(self._h, off.ctypes.data, nbr.ctypes.data if self.m else None,
                                       thr.ctypes.data if self.m else None, od.ctypes.data, idg.ctypes.data))
         return {"offsets": off, "nbr": nbr, "thresholds": thr, "out_deg": od, "in_deg": idg}
+
+    def degrees(self):
+        """(out_degree, in_degree) without copying the CSR itself."""
+        od = np.empty(self.v_num, np.uint32)
+        idg = np.empty(self.v_num, np.uint32)
+        check(lib().dg_graph_copy_csr(self._h, None, None, None, od.ctypes.data, idg.ctypes.data))
+        return od, idg
 
     def visits(self) -> np.ndarray:
         f = np.empty(self.v_num, np.uint32)

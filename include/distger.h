@@ -209,6 +209,49 @@ DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *ou
  * (word2vec.cu:1353-1362). */
 DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
 
+/* ------------------------- synthetic graphs and link prediction on device */
+
+/* The reference reads graphs from 12-byte edge files (storage.hpp:15-37) and
+ * splits them for link prediction on the host (src/tools/gtrain.cpp:226-386).
+ * These entry points generate, split, build and score on the device, for graphs
+ * too large for host tools (the Twitter-shaped workload: 41.6M vertices, 1.47B
+ * edges). */
+typedef struct {
+    uint32_t n;          /* vertices */
+    uint64_t m;          /* edge draws; self-loops and repeated pairs are dropped, isolated vertices get one edge */
+    double beta;         /* expected degrees proportional to (i + 1)^(-1/(beta - 1)) */
+    double max_degree;   /* cap on the expected degree (0: none) */
+    uint64_t seed;
+    int weighted;        /* 1: edge data uniform (0, 1]; 0: 1.0 */
+} dg_chung_lu_params;
+
+typedef struct dg_edges dg_edges;       /* undirected edge list on the device (unique pairs) */
+typedef struct dg_lp_pairs dg_lp_pairs; /* link-prediction test pairs on the device */
+
+/* Chung-Lu edge-sampling graph (deterministic in the seed). */
+DG_API int dg_edges_chung_lu(const dg_chung_lu_params *p, int device, dg_edges **out);
+DG_API int dg_edges_get_info(const dg_edges *e, uint32_t *v_num, uint64_t *n_edges);
+/* Host copy, pairs in ascending (src, dst) order with src < dst (each may be NULL). */
+DG_API int dg_edges_copy(const dg_edges *e, uint32_t *src, uint32_t *dst, float *data);
+DG_API void dg_edges_free(dg_edges *e);
+
+/* Holds out about frac of the edges (gtrain's rule in a parallel form: a
+ * hash-selected candidate stays in the graph when removing it would leave one of
+ * its endpoints without an edge) plus as many uniform non-edges of the full
+ * graph; the held-out edges leave `e`.  Test pairs: positives, then negatives. */
+DG_API int dg_edges_split(dg_edges *e, double frac, uint64_t seed, dg_lp_pairs **test);
+DG_API int dg_lp_pairs_get_info(const dg_lp_pairs *t, uint64_t *n_pos, uint64_t *n_neg);
+DG_API int dg_lp_pairs_copy(const dg_lp_pairs *t, uint32_t *u, uint32_t *v, uint8_t *label);
+DG_API void dg_lp_pairs_free(dg_lp_pairs *t);
+
+/* Undirected CSR of a device edge list, built on the device (both directions of
+ * every pair, rows sorted by neighbour, thresholds as for dg_graph_create). */
+DG_API int dg_graph_create_from_device_edges(const dg_edges *e, dg_graph **out);
+
+/* Link-prediction AUC of the trainer's input embedding on the test pairs: score
+ * sigmoid(v_u . v_v) (and cosine), Mann-Whitney AUC with ties averaged. */
+DG_API int dg_lp_auc(const dg_sgns *s, const dg_lp_pairs *t, double *auc, double *auc_cosine);
+
 /* -------------------------------------------------------------- autotuner */
 
 /* No counterpart in the reference (its kernels have fixed launches).  Each

@@ -163,6 +163,12 @@ int dgo_sgns_loss_grad(const double *in, const double *out, int d, uint32_t voca
                        int negative, int only_table, int64_t only_row, double *loss, double *grad_in,
                        double *grad_out);
 
+/* Device graph generator and link-prediction split, restated (dg_oracle_gen.c). */
+uint64_t dgo_chung_lu(uint32_t n, uint64_t m, double beta, double cap, uint64_t seed, uint64_t *keys);
+float dgo_edge_data(uint64_t key, uint64_t seed, int weighted);
+uint64_t dgo_lp_split(uint64_t *keys, uint64_t n, uint32_t v_num, double frac, uint64_t seed, uint32_t *pos_u,
+                      uint32_t *pos_v, uint32_t *neg_u, uint32_t *neg_v, uint64_t *n_pos);
+
 #ifdef __cplusplus
 }
 #endif

@@ -101,6 +101,13 @@ def lib():
         L.dgo_sgns_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.c_int64,
                                          C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dgo_chung_lu.argtypes = [C.c_uint32, C.c_uint64, C.c_double, C.c_double, C.c_uint64, C.c_void_p]
+        L.dgo_chung_lu.restype = C.c_uint64
+        L.dgo_edge_data.argtypes = [C.c_uint64, C.c_uint64, C.c_int]
+        L.dgo_edge_data.restype = C.c_float
+        L.dgo_lp_split.argtypes = [C.c_void_p, C.c_uint64, C.c_uint32, C.c_double, C.c_uint64, C.c_void_p, C.c_void_p,
+                                   C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dgo_lp_split.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -337,3 +344,27 @@ def sgns_loss_grad(in_rows: np.ndarray, out_rows: np.ndarray, inputs, outputs, n
     if rc:
         raise RuntimeError("dgo_sgns_loss_grad failed")
     return loss.value, gi, go
+
+
+def chung_lu_keys(n: int, m: int, beta: float, max_degree: float, seed: int) -> np.ndarray:
+    """Unique undirected pair keys (lo << 32 | hi) of the device generator, restated (dg_oracle_gen.c)."""
+    keys = np.zeros(m + n, np.uint64)
+    e = lib().dgo_chung_lu(n, m, beta, max_degree or 0.0, seed, keys.ctypes.data)
+    return keys[:e].copy()
+
+
+def edge_data(keys: np.ndarray, seed: int, weighted: bool) -> np.ndarray:
+    L = lib()
+    return np.array([L.dgo_edge_data(int(k), seed, int(weighted)) for k in keys.tolist()], np.float32)
+
+
+def lp_split(keys: np.ndarray, v_num: int, frac: float, seed: int):
+    """(kept keys, positives (u, v), negatives (u, v)) of the device split, restated."""
+    k = np.ascontiguousarray(keys, dtype=np.uint64).copy()
+    n = k.size
+    pu, pv, nu, nv = (np.zeros(max(n, 1), np.uint32) for _ in range(4))
+    npos = C.c_uint64()
+    nk = lib().dgo_lp_split(k.ctypes.data, n, v_num, frac, seed, pu.ctypes.data, pv.ctypes.data, nu.ctypes.data,
+                            nv.ctypes.data, C.byref(npos))
+    p = npos.value
+    return k[:nk], (pu[:p], pv[:p]), (nu[:p], nv[:p])

@@ -472,8 +472,10 @@ def run_auc_reference(args):
 
 # Graphs generated, split and built on the device (dg_edges_chung_lu, dg_edges_split,
 # dg_graph_create_from_device_edges); scored by dg_lp_auc.
+# C5: 2.417e9 draws leave ~1.47e9 unique undirected pairs (hub pairs repeat; measured
+# 2.3e9 -> 1.395e9, 2.7e9 -> 1.652e9 unique).
 SYNTH = {
-    "c5_twitter": dict(n=41_652_230, m=1_470_000_000, beta=1.9, max_degree=3_000_000.0, weighted=False,
+    "c5_twitter": dict(n=41_652_230, m=2_417_000_000, beta=1.9, max_degree=3_000_000.0, weighted=False,
                        holdout=0.01, min_r=5),
     "c2_youtube_device": dict(n=1_138_499, m=2_990_443, beta=2.1, max_degree=28_000.0, weighted=True,
                               holdout=0.1, min_r=5),

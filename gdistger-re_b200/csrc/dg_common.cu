@@ -32,6 +32,7 @@ void clear_error() { g_last_error.clear(); }
 static std::atomic<uint64_t> g_launches{0};
 
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 int sm_count(int device) {
     int n = 0;

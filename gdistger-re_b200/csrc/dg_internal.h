@@ -98,6 +98,7 @@ int sm_count(int device);
 
 // Counts kernel launches issued by this library (reported by dg_launch_count).
 void note_launch();
+void note_launches(uint64_t n);  // kernels run by a replayed CUDA graph
 
 // Exclusive prefix sum of n 32-bit counts into 64-bit offsets (out has n + 1
 // entries; out[n] = total).  Scratch is allocated internally.

@@ -672,7 +672,8 @@ dg_sgns::~dg_sgns() {
         v2w.release(); keep_thr.release(); table.release(); exp_table.release();
         syn0.release(); syn1.release(); in_bf.release(); out_bf.release(); in_master.release(); out_master.release();
         scratch.release(); queue.release(); stats.release(); adj_in.release(); adj_out.release(); adj_flag.release();
-        adj_offs.release(); adj_pin.release(); adj_pout.release(); adj_neg.release();
+        adj_offs.release(); adj_pin.release(); adj_pout.release(); adj_neg.release(); adj_step.release();
+        if (adj_exec) cudaGraphExecDestroy(adj_exec);
         cudaStreamDestroy(stream);
     }
 }

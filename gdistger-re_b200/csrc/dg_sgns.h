@@ -90,6 +90,15 @@ int adjoint_train(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
 uint32_t adjoint_step_bound(const std::vector<uint32_t> &cn, const std::vector<uint32_t> &keep_thr, int batch,
                             int negative);
 
+// Device-resident parameters of the adjoint mode's gradient steps.  The kernels
+// of a captured CUDA graph read the step index here (adj_advance moves it on),
+// so one instantiated graph of several steps serves every round.
+struct AdjStep {
+    uint64_t n_pairs, n_batches, k;  // k: minibatches per step
+    float alpha;
+    uint64_t step;
+};
+
 }  // namespace dgs
 
 struct dg_sgns {
@@ -119,6 +128,10 @@ struct dg_sgns {
     dg::DevArray<uint32_t> adj_pin, adj_pout, adj_neg;  // adjoint mode: pairs and shared negatives
     bool adj_dirty = false;                             // accumulators hold a finished gradient
     uint32_t adj_step_batches = 1;                      // adjoint mode: minibatches per gradient step
+    dg::DevArray<dgs::AdjStep> adj_step;                // adjoint mode: step parameters read by the graph
+    cudaGraphExec_t adj_exec = nullptr;                 // adjoint mode: kAdjGraphSteps steps, captured once
+    const void *adj_exec_key[3] = {nullptr, nullptr, nullptr};  // buffers the captured graph points at
+    uint64_t adj_exec_k = 0;
     dg::DevArray<uint32_t> queue;
     dg::DevArray<unsigned long long> stats;
     ~dg_sgns();

@@ -29,6 +29,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstring>
 
 namespace dgs {
 namespace {
@@ -38,10 +39,13 @@ constexpr float kFixScale = 1099511627776.0f;           // 2^40
 constexpr double kFixInv = 1.0 / 1099511627776.0;       // 2^-40
 constexpr float kFixMaxTerm = 1048576.0f;               // 2^20
 constexpr int kAdjThreads = 256;
+constexpr int kAdjGraphSteps = 16;                     // gradient steps per replayed graph
 
 struct AdjArgs {
-    const uint32_t *inputs, *outputs, *negatives;
+    const uint32_t *inputs, *outputs, *negatives;   // whole arrays, indexed by global pair / minibatch
     uint64_t n_pairs, n_batches;
+    uint64_t b_begin, b_end;                          // minibatches of this launch (when step is NULL)
+    const AdjStep *step;                              // else: the step's minibatches, read on the device
     uint32_t batch;
     int negative;
     const float *in_f32, *out_f32;              // plain form rows (else NULL)
@@ -98,9 +102,17 @@ __global__ void __launch_bounds__(kAdjThreads) sgns_adjoint_kernel(AdjArgs a) {
     const int neg = a.negative;
     float *uk = adj_smem + (size_t)wib * 2 * neg * D;   // [neg][D] negative rows
     float *gk = uk + (size_t)neg * D;                    // [neg][D] their gradient sums
+    uint64_t n_pairs = a.n_pairs, b_begin = a.b_begin, b_end = a.b_end;
+    if (a.step) {
+        const AdjStep st = *a.step;
+        n_pairs = st.n_pairs;
+        b_begin = st.step * st.k;
+        if (b_begin >= st.n_batches) return;   // a graph's steps past the round's end
+        b_end = min(b_begin + st.k, st.n_batches);
+    }
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
-    for (uint64_t b = (uint64_t)blockIdx.x * (blockDim.x / 32) + wib; b < a.n_batches; b += warps) {
-        const uint64_t p0 = b * a.batch, p1 = min(p0 + a.batch, a.n_pairs);
+    for (uint64_t b = b_begin + (uint64_t)blockIdx.x * (blockDim.x / 32) + wib; b < b_end; b += warps) {
+        const uint64_t p0 = b * a.batch, p1 = min(p0 + a.batch, n_pairs);
         for (int k = 0; k < neg; k++) {
             float x[V];
             adj_load<V>(a.out_f32, a.out_bf, a.out_master, a.n_master, a.negatives[b * neg + k], col, x);
@@ -189,16 +201,25 @@ __global__ void adj_negatives(const int32_t *table, uint64_t table_size, uint32_
 // accumulators for the next step.  A row that occurs several times is applied
 // once: the first visitor's exchange takes the whole sum, later ones read 0.
 // The step's contributions are complete when this kernel starts.
+// The step's minibatches [b0, b1) and pairs [p0, p1) come from the step record.
 __global__ void adjoint_apply_rows(unsigned long long *acc_in, unsigned long long *acc_out, const uint32_t *inputs,
-                                   const uint32_t *outputs, const uint32_t *negs, uint64_t n_pairs, uint64_t n_neg,
-                                   int d, float alpha, float *in_f32, float *out_f32, __nv_bfloat16 *in_bf,
+                                   const uint32_t *outputs, const uint32_t *negatives, uint32_t batch, int negative,
+                                   int d, const AdjStep *step, float *in_f32, float *out_f32, __nv_bfloat16 *in_bf,
                                    __nv_bfloat16 *out_bf, float *in_master, float *out_master, uint32_t n_master) {
+    const AdjStep st = *step;
+    const uint64_t b0 = st.step * st.k;
+    if (b0 >= st.n_batches) return;
+    const uint64_t b1 = min(b0 + st.k, st.n_batches);
+    const uint64_t p0 = b0 * batch, p1 = min(b1 * batch, st.n_pairs);
+    const uint64_t n_pairs = p1 - p0, n_neg = (b1 - b0) * (uint64_t)negative;
+    const uint32_t *in_ids = inputs + p0, *out_ids = outputs + p0, *negs = negatives + b0 * negative;
+    const float alpha = st.alpha;
     const uint64_t n = (2 * n_pairs + n_neg) * (uint64_t)d;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t occ = i / d;
         const uint32_t c = (uint32_t)(i % d);
         const bool input = occ < n_pairs;
-        const uint32_t row = input ? inputs[occ] : occ < 2 * n_pairs ? outputs[occ - n_pairs] : negs[occ - 2 * n_pairs];
+        const uint32_t row = input ? in_ids[occ] : occ < 2 * n_pairs ? out_ids[occ - n_pairs] : negs[occ - 2 * n_pairs];
         const uint64_t k = (uint64_t)row * d + c;
         const unsigned long long q = atomicExch(input ? acc_in + k : acc_out + k, 0ull);
         if (q == 0) continue;
@@ -214,6 +235,10 @@ __global__ void adjoint_apply_rows(unsigned long long *acc_in, unsigned long lon
             bf[k] = __float2bfloat16_rn(__fsub_rn(__bfloat162float(bf[k]), step));
         }
     }
+}
+
+__global__ void adj_advance(AdjStep *step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) step->step++;
 }
 
 __global__ void adjoint_to_f32(const unsigned long long *acc, uint64_t n, float *out) {
@@ -236,22 +261,77 @@ __global__ void adjoint_apply(const unsigned long long *acc, uint64_t n, float a
     }
 }
 
+// Launch geometry of the gradient kernel for up to n_batches minibatches per launch.
+struct AdjLaunch {
+    unsigned blocks = 1;
+    int threads = 32;
+    size_t smem = 0;
+};
+
 template <int V>
-int adjoint_launch(dg_sgns *s, const AdjArgs &a) {
-    const size_t per_warp = (size_t)2 * a.negative * 32 * V * sizeof(float);
+int adjoint_config(dg_sgns *s, int negative, uint64_t n_batches, AdjLaunch &l) {
+    const size_t per_warp = (size_t)2 * negative * 32 * V * sizeof(float);
     int warps = kAdjThreads / 32;
     while (warps > 1 && per_warp * warps > 96 * 1024) warps /= 2;
-    const size_t smem = per_warp * warps;
-    DG_CUDA(cudaFuncSetAttribute(sgns_adjoint_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    l.smem = per_warp * warps;
+    l.threads = warps * 32;
+    DG_CUDA(cudaFuncSetAttribute(sgns_adjoint_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
     int per_sm = 0;
-    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sgns_adjoint_kernel<V>, warps * 32, smem));
-    const uint64_t need = (a.n_batches + warps - 1) / warps;
-    const uint64_t blocks = std::max<uint64_t>(1, std::min<uint64_t>(need, (uint64_t)dg::sm_count(s->device) *
-                                                                              std::max(per_sm, 1)));
-    sgns_adjoint_kernel<V><<<(unsigned)blocks, warps * 32, smem, s->stream>>>(a);
-    dg::note_launch();
-    DG_CUDA(cudaGetLastError());
+    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sgns_adjoint_kernel<V>, l.threads, l.smem));
+    const uint64_t need = (n_batches + warps - 1) / warps;
+    l.blocks = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>(need, (uint64_t)dg::sm_count(s->device) * std::max(per_sm, 1)));
     return DG_OK;
+}
+
+int adjoint_configure(dg_sgns *s, int negative, uint64_t n_batches, AdjLaunch &l) {
+    switch (s->p.size) {
+    case 32: return adjoint_config<1>(s, negative, n_batches, l);
+    case 64: return adjoint_config<2>(s, negative, n_batches, l);
+    case 128: return adjoint_config<4>(s, negative, n_batches, l);
+    case 256: return adjoint_config<8>(s, negative, n_batches, l);
+    case 512: return adjoint_config<16>(s, negative, n_batches, l);
+    default: return dg::fail(DG_ERR_ARG, "size %d not supported", s->p.size);
+    }
+}
+
+// Kernel launch only (no runtime calls besides the launch: safe inside a stream capture).
+void adjoint_enqueue(dg_sgns *s, const AdjLaunch &l, const AdjArgs &a) {
+    switch (s->p.size) {
+    case 32: sgns_adjoint_kernel<1><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    case 64: sgns_adjoint_kernel<2><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    case 128: sgns_adjoint_kernel<4><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    case 256: sgns_adjoint_kernel<8><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    default: sgns_adjoint_kernel<16><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    }
+}
+
+AdjArgs adjoint_args(dg_sgns *s, const uint32_t *inputs, const uint32_t *outputs, const uint32_t *negatives,
+                     uint64_t n_pairs, uint32_t batch, int negative) {
+    AdjArgs a{};
+    a.inputs = inputs;
+    a.outputs = outputs;
+    a.negatives = negatives;
+    a.n_pairs = n_pairs;
+    a.n_batches = (n_pairs + batch - 1) / batch;
+    a.b_begin = 0;
+    a.b_end = a.n_batches;
+    a.step = nullptr;
+    a.batch = batch;
+    a.negative = negative;
+    const bool plain = s->p.mode == DG_SGNS_PLAIN;
+    a.in_f32 = plain ? s->syn0.p : nullptr;
+    a.out_f32 = plain ? s->syn1.p : nullptr;
+    a.in_bf = s->in_bf.p;
+    a.out_bf = s->out_bf.p;
+    a.in_master = s->in_master.p;
+    a.out_master = s->out_master.p;
+    a.n_master = plain ? 0 : s->n_master;
+    a.acc_in = s->adj_in.p;
+    a.acc_out = s->adj_out.p;
+    a.batch_loss = nullptr;
+    a.flag = s->adj_flag.p;
+    return a;
 }
 
 int adjoint_buffers(dg_sgns *s) {
@@ -271,34 +351,15 @@ int adjoint_grad(dg_sgns *s, const uint32_t *inputs, const uint32_t *outputs, co
                  uint64_t n_pairs, uint32_t batch, int negative, double *batch_loss) {
     const uint64_t n_batches = (n_pairs + batch - 1) / batch;
     if (n_batches == 0) return DG_OK;
-    AdjArgs a{};
-    a.inputs = inputs;
-    a.outputs = outputs;
-    a.negatives = negatives;
-    a.n_pairs = n_pairs;
-    a.n_batches = n_batches;
-    a.batch = batch;
-    a.negative = negative;
-    const bool plain = s->p.mode == DG_SGNS_PLAIN;
-    a.in_f32 = plain ? s->syn0.p : nullptr;
-    a.out_f32 = plain ? s->syn1.p : nullptr;
-    a.in_bf = s->in_bf.p;
-    a.out_bf = s->out_bf.p;
-    a.in_master = s->in_master.p;
-    a.out_master = s->out_master.p;
-    a.n_master = plain ? 0 : s->n_master;
-    a.acc_in = s->adj_in.p;
-    a.acc_out = s->adj_out.p;
+    AdjArgs a = adjoint_args(s, inputs, outputs, negatives, n_pairs, batch, negative);
     a.batch_loss = batch_loss;
-    a.flag = s->adj_flag.p;
-    switch (s->p.size) {
-    case 32: return adjoint_launch<1>(s, a);
-    case 64: return adjoint_launch<2>(s, a);
-    case 128: return adjoint_launch<4>(s, a);
-    case 256: return adjoint_launch<8>(s, a);
-    case 512: return adjoint_launch<16>(s, a);
-    default: return dg::fail(DG_ERR_ARG, "size %d not supported", s->p.size);
-    }
+    AdjLaunch l;
+    int rc = adjoint_configure(s, negative, n_batches, l);
+    if (rc) return rc;
+    adjoint_enqueue(s, l, a);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
 }
 
 // Uploads the pairs, clears the accumulators and runs the adjoint kernel.
@@ -405,19 +466,47 @@ int adjoint_train(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
         DG_CUDA(cudaGetLastError());
     }
     const uint64_t k = s->p.workers ? s->p.workers : s->adj_step_batches;
-    const bool plain = s->p.mode == DG_SGNS_PLAIN;
-    for (uint64_t b0 = 0; b0 < n_batches; b0 += k) {
-        const uint64_t nb = std::min<uint64_t>(k, n_batches - b0);
-        const uint64_t p0 = b0 * batch, p1 = std::min<uint64_t>(n_pairs, (b0 + nb) * batch);
-        rc = adjoint_grad(s, s->adj_pin.p + p0, s->adj_pout.p + p0, s->adj_neg.p + b0 * neg, p1 - p0, batch, neg,
-                          nullptr);
+    // Step parameters live on the device; the captured graph of kAdjGraphSteps
+    // steps (gradient, step, advance) reads them, so it is replayed as is every
+    // round and recaptured only when a buffer it points at moves.
+    if (s->adj_step.n == 0) DG_CUDA(s->adj_step.alloc(1));
+    const AdjStep h{n_pairs, n_batches, k, a.alpha, 0};
+    DG_CUDA(cudaMemcpyAsync(s->adj_step.p, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
+    const void *key[3] = {s->adj_pin.p, s->adj_pout.p, s->adj_neg.p};
+    if (!s->adj_exec || s->adj_exec_k != k || memcmp(key, s->adj_exec_key, sizeof(key)) != 0) {
+        if (s->adj_exec) {
+            cudaGraphExecDestroy(s->adj_exec);
+            s->adj_exec = nullptr;
+        }
+        const bool plain = s->p.mode == DG_SGNS_PLAIN;
+        AdjArgs ga = adjoint_args(s, s->adj_pin.p, s->adj_pout.p, s->adj_neg.p, 0, batch, neg);
+        ga.step = s->adj_step.p;
+        AdjLaunch l;
+        rc = adjoint_configure(s, neg, k, l);
         if (rc) return rc;
-        adjoint_apply_rows<<<grid, 256, 0, s->stream>>>(
-            s->adj_in.p, s->adj_out.p, s->adj_pin.p + p0, s->adj_pout.p + p0, s->adj_neg.p + b0 * neg, p1 - p0,
-            nb * neg, d, a.alpha, plain ? s->syn0.p : nullptr, plain ? s->syn1.p : nullptr, s->in_bf.p, s->out_bf.p,
-            s->in_master.p, s->out_master.p, plain ? 0u : s->n_master);
-        dg::note_launch();
-        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaStreamSynchronize(s->stream));
+        DG_CUDA(cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+        for (int i = 0; i < kAdjGraphSteps; i++) {
+            adjoint_enqueue(s, l, ga);
+            adjoint_apply_rows<<<grid, 256, 0, s->stream>>>(
+                s->adj_in.p, s->adj_out.p, s->adj_pin.p, s->adj_pout.p, s->adj_neg.p, batch, neg, d, s->adj_step.p,
+                plain ? s->syn0.p : nullptr, plain ? s->syn1.p : nullptr, s->in_bf.p, s->out_bf.p, s->in_master.p,
+                s->out_master.p, plain ? 0u : s->n_master);
+            adj_advance<<<1, 32, 0, s->stream>>>(s->adj_step.p);
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(s->stream, &graph);
+        DG_CUDA(ce);
+        const cudaError_t ie = cudaGraphInstantiate(&s->adj_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        DG_CUDA(ie);
+        memcpy(s->adj_exec_key, key, sizeof(key));
+        s->adj_exec_k = k;
+    }
+    const uint64_t n_steps = (n_batches + k - 1) / k;
+    for (uint64_t done = 0; done < n_steps; done += kAdjGraphSteps) {
+        DG_CUDA(cudaGraphLaunch(s->adj_exec, s->stream));
+        dg::note_launches(3 * kAdjGraphSteps);
     }
     unsigned int flag = 0;
     DG_CUDA(cudaMemcpyAsync(&flag, s->adj_flag.p, 4, cudaMemcpyDeviceToHost, s->stream));

@@ -52,6 +52,9 @@ struct MbArgs {
 
 // Warps per worker for a row size: each lane owns two columns (one for d = 32).
 constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
+// Workers per SM the register budget is sized for (shared memory allows about
+// as many): enough residency to reach the staleness bound on large vocabularies.
+constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 6 : 3; }
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
     h ^= h >> 16;
@@ -167,7 +170,7 @@ constexpr uint32_t mb_smem_bytes(int d, int out, int max_in, uint32_t pool_cap) 
 
 // D: row size; OUT: output slots per step (>= negative + 2, a divisor of 32).
 template <int D, int OUT>
-__global__ void __launch_bounds__(32 * mb_warps(D)) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
+__global__ void __launch_bounds__(32 * mb_warps(D), mb_min_blocks(D)) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
     constexpr int NW = mb_warps(D);
     constexpr int V = D / (32 * NW);
     constexpr int IPB = 32 / OUT;                   // inputs per batch of 32 corr dots
@@ -621,6 +624,8 @@ static int mb_setup(MbPlan &plan) {
     plan.threads = 32 * mb_warps(D);
     DG_CUDA(cudaFuncSetAttribute(sgns_mb_kernel<D, OUT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)plan.m.smem));
+    DG_CUDA(cudaFuncSetAttribute(sgns_mb_kernel<D, OUT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
     DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&plan.per_sm, sgns_mb_kernel<D, OUT>, plan.threads,
                                                           plan.m.smem));
     return DG_OK;

@@ -135,6 +135,7 @@ _SIGS = {
     "dg_lp_pairs_free": ([_P], None),
     "dg_graph_create_from_device_edges": ([_P, C.POINTER(_P)], C.c_int),
     "dg_lp_auc": ([_P, _P, C.POINTER(C.c_double), C.POINTER(C.c_double)], C.c_int),
+    "dg_common_neighbours": ([_P, _P, C.c_uint64, C.c_uint32, C.c_int, C.c_int, _P], C.c_int),
 }
 
 _lib = None

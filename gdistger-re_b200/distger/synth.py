@@ -108,3 +108,14 @@ class EdgeList:
             self.close()
         except Exception:
             pass
+
+
+def common_neighbours(src, dst, v_num: int, undirected: bool = True, device: int = 0) -> np.ndarray:
+    """Common-neighbour count of every edge (the reference's gcn tool, src/tools/gcn.cpp),
+    computed on the device by dg_common_neighbours; int32 in input order."""
+    s = np.ascontiguousarray(src, dtype=np.uint32)
+    d = np.ascontiguousarray(dst, dtype=np.uint32)
+    out = np.empty(s.size, np.int32)
+    check(lib().dg_common_neighbours(s.ctypes.data if s.size else None, d.ctypes.data if d.size else None, s.size,
+                                     v_num, int(undirected), device, out.ctypes.data if s.size else None))
+    return out

@@ -209,6 +209,21 @@ DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *ou
  * (word2vec.cu:1353-1362). */
 DG_API int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path);
 
+/* ------------------------------------------------------ common neighbours */
+
+/* Common-neighbour count of every edge, the edge data the HuGE transition reads
+ * (walk.hpp:920): replaces the reference's gcn tool (src/tools/gcn.cpp:249-373),
+ * computed on the device.  Rows are the CSR of the edges (both directions when
+ * undirected) sorted by neighbour, duplicates kept; for edge (s, d) the count is
+ * taken over the elements of the shorter row (N(s) on a tie) found in the other
+ * row, less one if the first is s or d and, when more than one remains, less one
+ * per later element that repeats its predecessor or is s or d (gcn.cpp:327-343);
+ * repeated pairs report the value of their first occurrence's orientation.  An
+ * empty row gives 0 (the tool reads past an empty row, directed inputs only).
+ * cn[n_edges] receives the counts in input order. */
+DG_API int dg_common_neighbours(const uint32_t *src, const uint32_t *dst, uint64_t n_edges, uint32_t v_num,
+                                int undirected, int device, int32_t *cn);
+
 /* ------------------------- synthetic graphs and link prediction on device */
 
 /* The reference reads graphs from 12-byte edge files (storage.hpp:15-37) and

@@ -368,3 +368,48 @@ def lp_split(keys: np.ndarray, v_num: int, frac: float, seed: int):
                             nv.ctypes.data, C.byref(npos))
     p = npos.value
     return k[:nk], (pu[:p], pv[:p]), (nu[:p], nv[:p])
+
+
+def common_neighbours(src, dst, v_num: int, undirected: bool = True) -> np.ndarray:
+    """Common-neighbour counts of the reference's gcn tool (src/tools/gcn.cpp:249-373), restated:
+    rows sorted by neighbour with duplicates (130-137); for edge (s, d) the elements of the shorter
+    row (N(s) on a tie, 166-172) found in the other row, with the shorter row's multiplicity; less
+    one if the first is s or d, and, when more than one remains, less one per later element that
+    repeats its predecessor or is s or d (327-343); a repeated pair reports its first occurrence's
+    value (305-310, 348-352).  An empty row gives 0."""
+    import bisect
+    src = np.asarray(src, dtype=np.int64)
+    dst = np.asarray(dst, dtype=np.int64)
+    a = np.concatenate([src, dst]) if undirected else src
+    b = np.concatenate([dst, src]) if undirected else dst
+    order = np.lexsort((b, a))
+    a, b = a[order], b[order]
+    offs = np.zeros(v_num + 1, np.int64)
+    np.add.at(offs, a + 1, 1)
+    offs = np.cumsum(offs)
+    rows = b.tolist()
+    seen = {}
+    out = np.zeros(src.size, np.int32)
+    for e, (s, d) in enumerate(zip(src.tolist(), dst.tolist())):
+        key = (min(s, d), max(s, d))
+        if key not in seen:
+            r1 = rows[offs[s]:offs[s + 1]]
+            r2 = rows[offs[d]:offs[d + 1]]
+            lg, sh = (r1, r2) if len(r1) > len(r2) else (r2, r1)
+            inter = []
+            if lg and sh:
+                for x in sh:
+                    i = bisect.bisect_left(lg, x)
+                    if i < len(lg) and lg[i] == x:
+                        inter.append(x)
+            cn = len(inter)
+            if cn > 0:
+                if inter[0] in (s, d):
+                    cn -= 1
+                if cn > 1:
+                    for i in range(1, len(inter)):
+                        if inter[i] == inter[i - 1] or inter[i] in (s, d):
+                            cn -= 1
+            seen[key] = cn
+        out[e] = seen[key]
+    return out

@@ -329,6 +329,9 @@ def run_ours(args, rank, world, local, pg):
     if train_ms >= walk_ms:
         kern = "sgns_plain" if mode == "plain" else "sgns_minibatch"
         alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else None
+        if mode == "plain_bf16":
+            # rows at 2 bytes (the 65,536 FP32 master rows are counted at 2 bytes too)
+            kern, alg = "sgns_plain_bf16", pairs * BYTES_PER_PAIR_PLAIN(128, 5) / 2
         if args.adjoint:
             kern = "sgns_adjoint pass (pair cut + gradient + step kernels)"
             alg = pairs * BYTES_PER_PAIR_ADJOINT(128, 5, 21, 4 if mode == "plain" else 2)
@@ -490,7 +493,10 @@ def run_auc_synth(args, local):
     from distger.synth import EdgeList
     torch.cuda.set_device(local)
     cfg = SYNTH[args.workload]
-    for form in args.auc_modes.split(","):
+    runs = [(f, 0) for f in args.auc_modes.split(",")]
+    if args.workers:
+        runs = [(f, int(w)) for f in args.auc_modes.split(",") for w in args.workers.split(",")]
+    for form, workers in runs:
         mode, _, variant = form.partition("-")
         t0 = time.perf_counter()
         e = EdgeList.chung_lu(cfg["n"], cfg["m"], cfg["beta"], seed=0, max_degree=cfg["max_degree"],
@@ -505,7 +511,8 @@ def run_auc_synth(args, local):
         clocks = Clocks(local)
         clocks.start()
         res = embed(graph, mode=mode, seed=args.seed, rounds=args.rounds, init_round=cfg["min_r"], max_len=32,
-                    deterministic=2 if variant == "adjoint" else 0, keep_trainer=True, device=local, **AUC_HP)
+                    deterministic=2 if variant == "adjoint" else 0, workers=workers, master_rows=args.master_rows,
+                    keep_trainer=True, device=local, **AUC_HP)
         clk = clocks.stop()
         t4 = time.perf_counter()
         sgns = res.pop("trainer")
@@ -513,6 +520,7 @@ def run_auc_synth(args, local):
         t5 = time.perf_counter()
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
                           "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16", "workers": res["workers"],
+                          "master_rows": args.master_rows,
                           "auc": m["auc"], "auc_cosine": m["auc_cosine"], "test_pairs": pairs.n_pos + pairs.n_neg,
                           "vertices": cfg["n"], "undirected_edges": n_edges, "rounds": len(res["rounds"]),
                           "generate_s": t1 - t0, "split_s": t2 - t1, "csr_build_s": t3 - t2,
@@ -550,6 +558,9 @@ def run_profile_case(args, local):
         s = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
                  min_count=0, mode="minibatch" if args.profile == "minibatch" else "plain", seed=1,
                  deterministic=2 if args.profile == "adjoint" else 0, device=local)
+        if args.profile == "sgns" and not args.no_autotune:
+            # 5 shapes x 2 timed launches come first: profile with `ncu -s 10` to skip them.
+            out["autotune"] = s.autotune(p2)
         info = s.train_paths(p2)
         out.update({"train_ms": info.train_ms, "pairs": info.pairs, "words": info.words})
         s.close()
@@ -567,7 +578,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["plain", "minibatch"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "plain_bf16", "minibatch"], default="plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")

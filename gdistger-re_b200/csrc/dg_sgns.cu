@@ -350,6 +350,208 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
     }
 }
 
+// ---------------------------------------------------- plain rule, BF16 rows
+
+__device__ __forceinline__ uint32_t bf_mix(uint32_t h) {
+    h ^= h >> 16;
+    h *= 0x7FEB352Du;
+    h ^= h >> 15;
+    h *= 0x846CA68Bu;
+    h ^= h >> 16;
+    return h;
+}
+
+// FP32 -> BF16 with stochastic rounding: 16 random bits added below the kept
+// mantissa, then truncation (unbiased in expectation; infinities and NaN kept).
+__device__ __forceinline__ uint16_t bf16_sr_bits(float x, uint32_t noise) {
+    uint32_t u = __float_as_uint(x);
+    if ((u & 0x7F800000u) != 0x7F800000u) u += noise & 0xFFFFu;
+    return (uint16_t)(u >> 16);
+}
+
+// A row of the BF16 tables: FP32 masters for ids < n_master, BF16 otherwise.
+// Lane l owns columns [l*VEC, l*VEC + VEC).
+template <int VEC>
+struct BfRows {
+    __nv_bfloat16 *bf;
+    float *master;
+    uint32_t n_master;
+    int d;
+    __device__ __forceinline__ void load(int32_t w, uint32_t lane, RowVec<VEC> &r) const {
+        if ((uint32_t)w < n_master) {
+            load_row<VEC>(master + (size_t)w * d + lane * VEC, r);
+            return;
+        }
+        const uint16_t *p = reinterpret_cast<const uint16_t *>(bf + (size_t)w * d + lane * VEC);
+        if constexpr (VEC == 8) {
+            const uint4 t = __ldcg(reinterpret_cast<const uint4 *>(p));
+            const uint32_t q[4] = {t.x, t.y, t.z, t.w};
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                r.v[2 * i] = __uint_as_float(q[i] << 16);
+                r.v[2 * i + 1] = __uint_as_float(q[i] & 0xFFFF0000u);
+            }
+        } else if constexpr (VEC == 4) {
+            const uint2 t = __ldcg(reinterpret_cast<const uint2 *>(p));
+            r.v[0] = __uint_as_float(t.x << 16);
+            r.v[1] = __uint_as_float(t.x & 0xFFFF0000u);
+            r.v[2] = __uint_as_float(t.y << 16);
+            r.v[3] = __uint_as_float(t.y & 0xFFFF0000u);
+        } else {
+            const uint32_t t = __ldcg(reinterpret_cast<const unsigned int *>(p));
+            r.v[0] = __uint_as_float(t << 16);
+            r.v[1] = __uint_as_float(t & 0xFFFF0000u);
+        }
+    }
+    // One hash per row write; each 32-bit word of noise rounds two elements, the
+    // next word comes from one LCG step.
+    __device__ __forceinline__ void store_bits(int32_t w, uint32_t lane, const RowVec<VEC> &r, uint32_t salt) const {
+        uint16_t h[VEC];
+        uint32_t x = bf_mix(salt);
+#pragma unroll
+        for (int i = 0; i < VEC; i += 2) {
+            h[i] = bf16_sr_bits(r.v[i], x);
+            h[i + 1] = bf16_sr_bits(r.v[i + 1], x >> 16);
+            x = x * 0x9E3779B1u + 0x7F4A7C15u;
+        }
+        uint16_t *p = reinterpret_cast<uint16_t *>(bf + (size_t)w * d + lane * VEC);
+        if constexpr (VEC == 8) {
+            uint4 t;
+            t.x = h[0] | ((uint32_t)h[1] << 16);
+            t.y = h[2] | ((uint32_t)h[3] << 16);
+            t.z = h[4] | ((uint32_t)h[5] << 16);
+            t.w = h[6] | ((uint32_t)h[7] << 16);
+            __stcg(reinterpret_cast<uint4 *>(p), t);
+        } else if constexpr (VEC == 4) {
+            uint2 t;
+            t.x = h[0] | ((uint32_t)h[1] << 16);
+            t.y = h[2] | ((uint32_t)h[3] << 16);
+            __stcg(reinterpret_cast<uint2 *>(p), t);
+        } else {
+            __stcg(reinterpret_cast<unsigned int *>(p), (unsigned int)(h[0] | ((uint32_t)h[1] << 16)));
+        }
+    }
+    // Hogwild write of an updated row: FP32 masters (the hottest rows, where
+    // writers collide) receive `delta` by vector atomics; a BF16 row is stored
+    // as the warp's updated copy `value` (loaded at the start of the pair, so an
+    // update another warp made to the same cold row in that window is lost, as
+    // in any Hogwild scheme), rounded stochastically -- a store, not a
+    // read-modify-write, so the warp does not wait on it.
+    __device__ __forceinline__ void update(int32_t w, uint32_t lane, const RowVec<VEC> &delta,
+                                           const RowVec<VEC> &value, uint32_t salt) const {
+        if ((uint32_t)w < n_master) add_row<VEC>(master + (size_t)w * d + lane * VEC, delta);
+        else store_bits(w, lane, value, salt);
+    }
+    // row = value (one writer: deterministic mode).
+    __device__ __forceinline__ void put(int32_t w, uint32_t lane, const RowVec<VEC> &v, uint32_t salt) const {
+        if ((uint32_t)w < n_master) store_row<VEC>(master + (size_t)w * d + lane * VEC, v);
+        else store_bits(w, lane, v, salt);
+    }
+};
+
+// The plain kernel's schedule and update rule (word2vec.cu:305-399) on BF16
+// rows: the same pairs, draws and update order as sgns_plain_kernel, arithmetic
+// in FP32; each row write rounds stochastically with noise keyed by
+// (row, walk, centre, slot), so a deterministic run is reproducible.
+template <int VEC, int THREADS>
+__global__ void __launch_bounds__(THREADS) sgns_plain_bf16_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    const int d = 32 * VEC;
+    const float alpha = a.alpha;
+    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    const BfRows<VEC> in{a.in_bf, a.in_master, a.n_master, d};
+    const BfRows<VEC> out{a.out_bf, a.out_master, a.n_master, d};
+    const uint32_t key = a.seed_lo ^ bf_mix(a.pass * 0x9E3779B9u + 0x2F6B3A91u);
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % (uint32_t)a.window;
+            // Row noise: distinct per (walk, centre, slot, row, lane).
+            const uint32_t base = bf_mix(key ^ bf_mix(wid * 0x01000193u + p * 0x2545F491u) ^ lane * 0x85EBCA6Bu);
+            RowVec<VEC> pos, pos0;
+            out.load(word, lane, pos);
+            pos0 = pos;
+            for (uint32_t s = b; s < (uint32_t)(2 * a.window + 1) - b; s++) {
+                if (s == (uint32_t)a.window) continue;
+                const int64_t c = (int64_t)p - a.window + s;
+                if (c < 0 || c >= (int64_t)n) continue;
+                const int32_t last = sen[c];
+                int32_t my_t = -1;
+                if ((int)lane < neg) my_t = negative_target(a, p, s, wid, (int)lane + 1);
+                int32_t t[kFastNeg];
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++) t[j] = __shfl_sync(0xffffffffu, my_t, j);
+                RowVec<VEC> l1, e, l2[kFastNeg];
+                in.load(last, lane, l1);
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++)
+                    if (j < neg && t[j] != word) out.load(t[j], lane, l2[j]);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
+                n_pairs++;
+                {
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < kFastNeg; j++) {
+                    if (j >= neg || t[j] == word) continue;
+                    const float g = sg_grad(warp_dot<VEC>(l1, l2[j]), 0, a.exp_table, alpha);
+                    RowVec<VEC> upd;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, l2[j].v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, l1.v[i]);
+                        l2[j].v[i] += upd.v[i];
+                    }
+                    const uint32_t salt = base + (uint32_t)t[j] * 0x27D4EB2Fu + s * 16u + (uint32_t)j;
+                    if (a.deterministic) out.put(t[j], lane, l2[j], salt);
+                    else out.update(t[j], lane, upd, l2[j], salt);
+#pragma unroll
+                    for (int k = j + 1; k < kFastNeg; k++)
+                        if (t[k] == t[j]) l2[k] = l2[j];
+                }
+                const uint32_t salt1 = base + (uint32_t)last * 0x165667B1u + s * 16u + 15u;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
+                if (a.deterministic) in.put(last, lane, l1, salt1);
+                else in.update(last, lane, e, l1, salt1);
+            }
+            const uint32_t salt0 = base + (uint32_t)word * 0xD3A2646Cu + 0x5BD1E995u;
+            if (a.deterministic) {
+                out.put(word, lane, pos, salt0);
+            } else {
+                RowVec<VEC> delta;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) delta.v[i] = pos.v[i] - pos0.v[i];
+                out.update(word, lane, delta, pos, salt0);
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
 // One target at a time (any negative count up to 64).
 template <int VEC>
 __global__ void __launch_bounds__(kPlainThreads) sgns_plain_seq_kernel(SgnsArgs a, WalkSet ws) {
@@ -566,36 +768,56 @@ static int plain_blocks(const dg_sgns *s, int resident, int threads) {
 
 // One launch of the fast plain kernel in launch shape I (threads per block,
 // blocks per SM); dg_sgns_autotune picks the shape.
-template <int V, int I>
+template <int V, int I, bool BF>
 static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     constexpr int T = kPlainShapes[I].threads;
     int blocks = 1, threads = 32;
+    void (*kern)(SgnsArgs, WalkSet);
+    if constexpr (BF) kern = sgns_plain_bf16_kernel<V, T>;
+    else kern = sgns_plain_kernel<V, T>;
     if (!s->p.deterministic) {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sgns_plain_kernel<V, T>, T, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
         per_sm = std::max(per_sm, 1);
         if (kPlainShapes[I].per_sm > 0) per_sm = std::min(per_sm, kPlainShapes[I].per_sm);
         blocks = plain_blocks(s, dg::sm_count(s->device) * per_sm, T);
         threads = T;
     }
-    sgns_plain_kernel<V, T><<<blocks, threads, 0, s->stream>>>(a, ws);
+    kern<<<blocks, threads, 0, s->stream>>>(a, ws);
 }
 
-template <int V>
+template <int V, bool BF>
 static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     static_assert(kPlainShapeCount == 5, "dispatch below lists every shape");
     switch (s->plain_shape) {
-    case 0: plain_fast_launch<V, 0>(s, a, ws); break;
-    case 1: plain_fast_launch<V, 1>(s, a, ws); break;
-    case 2: plain_fast_launch<V, 2>(s, a, ws); break;
-    case 3: plain_fast_launch<V, 3>(s, a, ws); break;
-    case 4: plain_fast_launch<V, 4>(s, a, ws); break;
+    case 0: plain_fast_launch<V, 0, BF>(s, a, ws); break;
+    case 1: plain_fast_launch<V, 1, BF>(s, a, ws); break;
+    case 2: plain_fast_launch<V, 2, BF>(s, a, ws); break;
+    case 3: plain_fast_launch<V, 3, BF>(s, a, ws); break;
+    case 4: plain_fast_launch<V, 4, BF>(s, a, ws); break;
     default: return dg::fail(DG_ERR_ARG, "plain launch shape %d out of range", s->plain_shape);
     }
     return DG_OK;
 }
 
+// The plain rule on BF16 rows (DG_SGNS_PLAIN_BF16): size 64, 128 or 256, negative <= kFastNeg.
+static int launch_plain_bf16(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    DG_CHECK(a.negative <= kFastNeg, DG_ERR_ARG, "the BF16 plain trainer supports negative <= %d", kFastNeg);
+    int rc;
+    switch (s->p.size) {
+    case 64: rc = plain_fast_shape<2, true>(s, a, ws); break;
+    case 128: rc = plain_fast_shape<4, true>(s, a, ws); break;
+    case 256: rc = plain_fast_shape<8, true>(s, a, ws); break;
+    default: return dg::fail(DG_ERR_ARG, "the BF16 plain trainer supports size 64, 128 or 256 (got %d)", s->p.size);
+    }
+    if (rc) return rc;
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    if (s->p.mode == DG_SGNS_PLAIN_BF16) return launch_plain_bf16(s, a, ws);
     const int vec = s->p.size / 32;
     int blocks = 1, threads = 32;
     auto occ = [&](auto kern) {
@@ -609,7 +831,7 @@ int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 #define DG_PLAIN_CASE(V)                                                                             \
     case V:                                                                                          \
         if (fast) {                                                                                  \
-            int rc_ = plain_fast_shape<V>(s, a, ws);                                                 \
+            int rc_ = plain_fast_shape<V, false>(s, a, ws);                                          \
             if (rc_) return rc_;                                                                     \
         } else {                                                                                     \
             if (!s->p.deterministic)                                                                 \
@@ -688,7 +910,10 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
              DG_ERR_ARG, "size %d not supported (32, 64, 128, 256 or 512)", p->size);
     DG_CHECK(p->window >= 1 && p->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", p->window);
     DG_CHECK(p->negative >= 0 && p->negative <= 64, DG_ERR_ARG, "negative %d out of range [0, 64]", p->negative);
-    DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH, DG_ERR_ARG, "unknown mode %d", p->mode);
+    DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH || p->mode == DG_SGNS_PLAIN_BF16, DG_ERR_ARG,
+             "unknown mode %d", p->mode);
+    DG_CHECK(p->mode != DG_SGNS_PLAIN_BF16 || ((p->size == 64 || p->size == 128 || p->size == 256) && p->negative <= 8),
+             DG_ERR_ARG, "the BF16 plain trainer supports size 64, 128 or 256 and negative <= 8");
     DG_CHECK(p->iter >= 1, DG_ERR_ARG, "iter must be >= 1");
     DG_CHECK(p->deterministic >= 0 && p->deterministic <= 2, DG_ERR_ARG, "deterministic must be 0, 1 or 2");
     DG_CHECK(p->deterministic != 2 || p->negative <= 16, DG_ERR_ARG, "adjoint mode supports negative <= 16");
@@ -794,7 +1019,7 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
             rc = adjoint_train(s, a, ws, np);
             adj_pairs += np;
         } else {
-            rc = s->p.mode == DG_SGNS_PLAIN ? launch_plain(s, a, ws) : launch_minibatch(s, a, ws);
+            rc = s->p.mode == DG_SGNS_MINIBATCH ? launch_minibatch(s, a, ws) : launch_plain(s, a, ws);
         }
         if (rc) return rc;
     }
@@ -823,24 +1048,33 @@ extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alph
 extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info *info) {
     DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_autotune: NULL argument");
     dg_tune_info r{};
-    if (s->p.mode != DG_SGNS_PLAIN || s->p.deterministic || s->p.negative > dgs::kFastNeg) {
+    if (s->p.mode == DG_SGNS_MINIBATCH || s->p.deterministic || s->p.negative > dgs::kFastNeg) {
         r.n_candidates = 1;
         r.chosen = 0;
         if (info) *info = r;
         return DG_OK;
     }
     dg::DeviceGuard guard(s->device);
-    const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
-    dg::DevArray<float> s0, s1;
-    DG_CUDA(s0.alloc(n));
-    DG_CUDA(s1.alloc(n));
-    DG_CUDA(cudaMemcpyAsync(s0.p, s->syn0.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
-    DG_CUDA(cudaMemcpyAsync(s1.p, s->syn1.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+    // Snapshots of every row buffer the trainer holds (FP32 rows, or BF16 rows + masters).
+    struct Snap {
+        void *dev;
+        size_t bytes;
+        dg::DevArray<uint8_t> copy;
+    };
+    Snap snaps[6] = {{s->syn0.p, s->syn0.bytes(), {}},       {s->syn1.p, s->syn1.bytes(), {}},
+                     {s->in_bf.p, s->in_bf.bytes(), {}},     {s->out_bf.p, s->out_bf.bytes(), {}},
+                     {s->in_master.p, s->in_master.bytes(), {}}, {s->out_master.p, s->out_master.bytes(), {}}};
+    for (Snap &sn : snaps) {
+        if (!sn.dev || !sn.bytes) continue;
+        DG_CUDA(sn.copy.alloc(sn.bytes));
+        DG_CUDA(cudaMemcpyAsync(sn.copy.p, sn.dev, sn.bytes, cudaMemcpyDeviceToDevice, s->stream));
+    }
     const uint32_t pass0 = s->pass;
     const int shape0 = s->plain_shape;
     auto restore = [&]() -> int {
-        DG_CUDA(cudaMemcpyAsync(s->syn0.p, s0.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
-        DG_CUDA(cudaMemcpyAsync(s->syn1.p, s1.p, n * 4, cudaMemcpyDeviceToDevice, s->stream));
+        for (Snap &sn : snaps)
+            if (sn.dev && sn.bytes)
+                DG_CUDA(cudaMemcpyAsync(sn.dev, sn.copy.p, sn.bytes, cudaMemcpyDeviceToDevice, s->stream));
         DG_CUDA(cudaStreamSynchronize(s->stream));
         s->pass = pass0;
         return DG_OK;

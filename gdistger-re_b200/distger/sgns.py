@@ -17,7 +17,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 
-MODES = {"plain": 0, "minibatch": 1}
+MODES = {"plain": 0, "minibatch": 1, "plain_bf16": 2}
 
 
 class SGNS:

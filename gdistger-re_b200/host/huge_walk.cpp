@@ -20,7 +20,8 @@
 //   -threads / -debug / -reuse-neg: accepted, no effect on one GPU
 //   -hs, -cbow, -binary: only 0 is supported (skip-gram, negative sampling, text)
 // Added for the GPU build:
-//   -mode plain|minibatch   trainer form (default plain = word2vec.cu semantics)
+//   -mode plain|plain_bf16|minibatch   trainer form (default plain = word2vec.cu semantics
+//                           on FP32 rows; plain_bf16: the same rule on BF16 rows)
 //   -lr exp|fixed|cosine|step|custom   per-round schedule (default exp, decay 0.1)
 //   -rounds n               stop after round n (default 30)
 //   -train-from n           first round whose walks are trained (default 1;
@@ -123,7 +124,8 @@ Options parse(int argc, char **argv) {
         die("usage: huge_walk -g edges.bin -v V -w W [--min_L L] [--min_R R] [--make-undirected] [-o prefix] "
             "[-size d -window k -negative n -batch-size b -sample s -alpha a -iter i -min-count c "
             "-emb_output file] [-mode plain|minibatch]");
-    if (o.mode != "plain" && o.mode != "minibatch") die("-mode must be plain or minibatch");
+    if (o.mode != "plain" && o.mode != "minibatch" && o.mode != "plain_bf16")
+        die("-mode must be plain, plain_bf16 or minibatch");
     if (o.rounds < 1 || o.rounds > 30) die("-rounds must be 1..30 (walk.hpp:740 stops after round 30)");
     return o;
 }
@@ -171,7 +173,7 @@ int main(int argc, char **argv) {
     sp.alpha = o.alpha;
     sp.iter = o.iter;
     sp.min_count = o.min_count;
-    sp.mode = o.mode == "plain" ? DG_SGNS_PLAIN : DG_SGNS_MINIBATCH;
+    sp.mode = o.mode == "plain" ? DG_SGNS_PLAIN : o.mode == "plain_bf16" ? DG_SGNS_PLAIN_BF16 : DG_SGNS_MINIBATCH;
     sp.deterministic = o.deterministic;
     sp.seed = o.seed;
     sp.table_size = o.table_size;

@@ -131,6 +131,9 @@ DG_API int dg_graph_copy_visits(const dg_graph *g, uint32_t *freq);
 enum {
     DG_SGNS_PLAIN = 0,      /* word2vec.cu skip_gram_kernel semantics: FP32 rows, per-pair negatives, Hogwild */
     DG_SGNS_MINIBATCH = 1,  /* dsgl.hpp Train_SGNS_MPI semantics: shared negatives, BF16 rows, FP32 accumulation */
+    DG_SGNS_PLAIN_BF16 = 2, /* the plain (word2vec.cu) rule on BF16 rows: FP32 arithmetic, FP32 master rows for
+                               the hottest words (atomics), stochastic rounding for the rest; negative <= 8,
+                               size 64, 128 or 256 */
 };
 
 typedef struct {

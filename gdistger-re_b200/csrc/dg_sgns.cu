@@ -250,13 +250,42 @@ __device__ __forceinline__ int32_t negative_target(const SgnsArgs &a, uint32_t p
 // repeats an earlier one of the same pair is re-read from the updated copy.
 // Handles negative <= kFastNeg; larger counts use sgns_plain_seq_kernel.
 constexpr int kFastNeg = 8;
+constexpr uint32_t kSlotChunk = 32;   // window slots whose negatives are drawn together
+
+// Draws the negatives of window slots [cs, ce) of centre p into tb (kFastNeg per
+// slot), all lanes at once, so that the pairs of a centre wait on the unigram
+// table once instead of once per pair.  The draws are the per-pair draws
+// (negative_target), so the result is unchanged.  Slot == window is skipped.
+__device__ __forceinline__ void draw_negatives(const SgnsArgs &a, uint32_t p, uint32_t wid, uint32_t cs, uint32_t ce,
+                                               int neg, int32_t *tb) {
+    const uint32_t lane = threadIdx.x & 31;
+    __syncwarp();
+    const uint32_t total = (ce - cs) * (uint32_t)neg;
+    for (uint32_t q = lane; q < total; q += 32) {
+        const uint32_t k = q / (uint32_t)neg, j = q % (uint32_t)neg;
+        const uint32_t s = cs + k;
+        if (s == (uint32_t)a.window) continue;
+        tb[k * kFastNeg + j] = negative_target(a, p, s, wid, (int)j + 1);
+    }
+    __syncwarp();
+}
+
+// Window slots of centre p whose context lies inside the sentence:
+// [max(b, w - p), min(2w + 1 - b, n + w - p)), slot w excluded by the caller.
+__device__ __forceinline__ void slot_range(uint32_t p, uint32_t n, uint32_t w, uint32_t b, uint32_t &lo,
+                                           uint32_t &hi) {
+    lo = max(b, w > p ? w - p : 0u);
+    hi = min(2 * w + 1 - b, n + w - p);
+}
 
 template <int VEC, int THREADS>
 __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
+    __shared__ int32_t tb_all[THREADS / 32][kSlotChunk * kFastNeg];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
     int32_t *sen = sen_all[warp];
+    int32_t *tb = tb_all[warp];
     const int d = 32 * VEC;
     const float alpha = a.alpha;
     const int neg = a.vocab_size > 1 ? a.negative : 0;
@@ -278,18 +307,19 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
             RowVec<VEC> pos, pos0;
             load_row<VEC>(pos_row, pos);
             pos0 = pos;
-            for (uint32_t s = b; s < (uint32_t)(2 * a.window + 1) - b; s++) {
+            uint32_t s_lo, s_hi;
+            slot_range(p, n, (uint32_t)a.window, b, s_lo, s_hi);
+            for (uint32_t cs = s_lo; cs < s_hi; cs += kSlotChunk) {
+            const uint32_t ce = min(cs + kSlotChunk, s_hi);
+            draw_negatives(a, p, wid, cs, ce, neg, tb);
+            for (uint32_t s = cs; s < ce; s++) {
                 if (s == (uint32_t)a.window) continue;
                 const int64_t c = (int64_t)p - a.window + s;
-                if (c < 0 || c >= (int64_t)n) continue;
                 const int32_t last = sen[c];
                 float *l1p = a.syn0 + (size_t)last * d + lane * VEC;
-                // Lane j - 1 draws negative j; everyone learns all targets.
-                int32_t my_t = -1;
-                if ((int)lane < neg) my_t = negative_target(a, p, s, wid, (int)lane + 1);
                 int32_t t[kFastNeg];
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) t[j] = __shfl_sync(0xffffffffu, my_t, j);
+                for (int j = 0; j < kFastNeg; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
                 // Issue every row load of the pair before consuming any.
                 RowVec<VEC> l1, e, l2[kFastNeg];
                 load_row<VEC>(l1p, l1);
@@ -333,6 +363,7 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
                 } else {
                     add_row<VEC>(l1p, e);
                 }
+            }
             }
             if (a.deterministic) {
                 store_row<VEC>(pos_row, pos);
@@ -456,9 +487,11 @@ struct BfRows {
 template <int VEC, int THREADS>
 __global__ void __launch_bounds__(THREADS) sgns_plain_bf16_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
+    __shared__ int32_t tb_all[THREADS / 32][kSlotChunk * kFastNeg];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t warp = threadIdx.x >> 5;
     int32_t *sen = sen_all[warp];
+    int32_t *tb = tb_all[warp];
     const int d = 32 * VEC;
     const float alpha = a.alpha;
     const int neg = a.vocab_size > 1 ? a.negative : 0;
@@ -484,16 +517,18 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_bf16_kernel(SgnsArgs a, Wa
             RowVec<VEC> pos, pos0;
             out.load(word, lane, pos);
             pos0 = pos;
-            for (uint32_t s = b; s < (uint32_t)(2 * a.window + 1) - b; s++) {
+            uint32_t s_lo, s_hi;
+            slot_range(p, n, (uint32_t)a.window, b, s_lo, s_hi);
+            for (uint32_t cs = s_lo; cs < s_hi; cs += kSlotChunk) {
+            const uint32_t ce = min(cs + kSlotChunk, s_hi);
+            draw_negatives(a, p, wid, cs, ce, neg, tb);
+            for (uint32_t s = cs; s < ce; s++) {
                 if (s == (uint32_t)a.window) continue;
                 const int64_t c = (int64_t)p - a.window + s;
-                if (c < 0 || c >= (int64_t)n) continue;
                 const int32_t last = sen[c];
-                int32_t my_t = -1;
-                if ((int)lane < neg) my_t = negative_target(a, p, s, wid, (int)lane + 1);
                 int32_t t[kFastNeg];
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) t[j] = __shfl_sync(0xffffffffu, my_t, j);
+                for (int j = 0; j < kFastNeg; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
                 RowVec<VEC> l1, e, l2[kFastNeg];
                 in.load(last, lane, l1);
 #pragma unroll
@@ -533,6 +568,7 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_bf16_kernel(SgnsArgs a, Wa
                 for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
                 if (a.deterministic) in.put(last, lane, l1, salt1);
                 else in.update(last, lane, e, l1, salt1);
+            }
             }
             const uint32_t salt0 = base + (uint32_t)word * 0xD3A2646Cu + 0x5BD1E995u;
             if (a.deterministic) {

@@ -559,7 +559,7 @@ def run_profile_case(args, local):
                  min_count=0, mode="minibatch" if args.profile == "minibatch" else "plain", seed=1,
                  deterministic=2 if args.profile == "adjoint" else 0, device=local)
         if args.profile == "sgns" and not args.no_autotune:
-            # 5 shapes x 2 timed launches come first: profile with `ncu -s 10` to skip them.
+            # 7 shapes x 2 timed launches come first: profile with `ncu -s 14` to skip them.
             out["autotune"] = s.autotune(p2)
         info = s.train_paths(p2)
         out.update({"train_ms": info.train_ms, "pairs": info.pairs, "words": info.words})

@@ -182,17 +182,53 @@ __device__ __forceinline__ float warp_dot(const RowVec<VEC> &a, const RowVec<VEC
     float s = 0.f;
 #pragma unroll
     for (int i = 0; i < VEC; i++) s = fmaf(a.v[i], b.v[i], s);
+    // Butterfly: lanes i and i^o add the same two values (in swapped order, which
+    // float addition does not see), so every lane ends with the same sum.
 #pragma unroll
     for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return __shfl_sync(0xffffffffu, s, 0);  // one value for every lane
+    return s;
 }
+
+// Warp sums of M per-lane partials v[0..M) (M a power of two <= 32) for the cost
+// of about one: each halving stage sends half of the values still held to the
+// partner lane and keeps the other half, so after log2(M) stages lane l holds
+// one value, index l >> (5 - log2 M), summed over its lane group; plain
+// butterfly stages finish it.  Every addition is the one warp_dot's butterfly
+// makes for that value (own partial + partner's, then the same tree), so each
+// sum is bit-identical to warp_dot's.  Returns the held sum; v is clobbered.
+template <int M>
+__device__ __forceinline__ float warp_sums_split(float (&v)[M], uint32_t lane) {
+    static_assert(M >= 1 && M <= 32 && (M & (M - 1)) == 0, "M must be a power of two <= 32");
+#pragma unroll
+    for (int m = M, o = 16; m > 1; m >>= 1, o >>= 1) {
+        const bool up = (lane & (uint32_t)o) != 0;
+#pragma unroll
+        for (int k = 0; k < m / 2; k++) {
+            const float send = up ? v[k] : v[k + m / 2];
+            const float keep = up ? v[k + m / 2] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    float s = v[0];
+#pragma unroll
+    for (int o = 16 / M; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : 2 * pow2_at_least((x + 1) / 2); }
 
 // g = (label - sigmoid(f)) * alpha through expTable (word2vec.cu:383-388), with
 // the reference's integer-division index scale (EXP_TABLE_SIZE / MAX_EXP / 2 = 83).
 __device__ __forceinline__ float sg_grad(float f, int label, const float *exp_table, float alpha) {
     if (f > kMaxExp) return (label - 1) * alpha;
     if (f < -kMaxExp) return label * alpha;
-    return (label - exp_table[(int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2))]) * alpha;
+    return (label - __ldg(exp_table + (int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2)))) * alpha;
+}
+
+// Brings [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte aligned).  A
+// hint only: it holds no registers and orders nothing.
+__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(bytes));
 }
 
 __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
@@ -278,8 +314,17 @@ __device__ __forceinline__ void slot_range(uint32_t p, uint32_t n, uint32_t w, u
     hi = min(2 * w + 1 - b, n + w - p);
 }
 
-template <int VEC, int THREADS>
-__global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
+// Pairs ahead whose rows are prefetched into L2 while the current pair runs.
+constexpr uint32_t kPrefetchPairs = 2;
+// Negative count with its own compile-time instance (word2vec's and DistGER's default).
+constexpr int kPlainNeg = 5;
+
+// NEG > 0: the negative count fixed at compile time (a.negative == NEG, vocabulary
+// of more than one word); NEG == 0: any count <= kFastNeg read from a.negative.
+// FIT > 0: registers capped so that FIT blocks fit on an SM.
+template <int VEC, int THREADS, int NEG, int FIT>
+__global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(SgnsArgs a, WalkSet ws) {
+    constexpr int NS = NEG > 0 ? NEG : kFastNeg;   // negative slots held in registers
     __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
     __shared__ int32_t tb_all[THREADS / 32][kSlotChunk * kFastNeg];
     const uint32_t lane = threadIdx.x & 31;
@@ -287,8 +332,9 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
     int32_t *sen = sen_all[warp];
     int32_t *tb = tb_all[warp];
     const int d = 32 * VEC;
+    const uint32_t w = (uint32_t)a.window;
     const float alpha = a.alpha;
-    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    const int neg = NEG > 0 ? NEG : (a.vocab_size > 1 ? a.negative : 0);
     unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
     for (;;) {
         uint32_t walk = 0;
@@ -300,35 +346,127 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
         const uint32_t n = warp_sentence(ws, walk, a, sen, words);
         n_words += words;
         n_trained += n;
+        uint32_t b_next = philox(0, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
         for (uint32_t p = 0; p < n; p++) {
             const int32_t word = sen[p];
-            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % (uint32_t)a.window;
+            const uint32_t b = b_next;
             float *pos_row = a.syn1 + (size_t)word * d + lane * VEC;
             RowVec<VEC> pos, pos0;
             load_row<VEC>(pos_row, pos);
             pos0 = pos;
             uint32_t s_lo, s_hi;
-            slot_range(p, n, (uint32_t)a.window, b, s_lo, s_hi);
+            slot_range(p, n, w, b, s_lo, s_hi);
+            // Slot w lies in [s_lo, s_hi) (s_lo <= w < s_hi since p < n), so the
+            // centre has s_hi - s_lo - 1 pairs; likewise the next centre.
+            const uint32_t n_pairs_here = s_hi - s_lo - 1;
+            uint32_t q_lo = 0, q_hi = 0;
+            if (p + 1 < n) {
+                b_next = philox(p + 1, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
+                slot_range(p + 1, n, w, b_next, q_lo, q_hi);
+                if (lane == 0) prefetch_l2(a.syn1 + (size_t)sen[p + 1] * d, (uint32_t)d * 4);
+            }
             for (uint32_t cs = s_lo; cs < s_hi; cs += kSlotChunk) {
             const uint32_t ce = min(cs + kSlotChunk, s_hi);
             draw_negatives(a, p, wid, cs, ce, neg, tb);
             for (uint32_t s = cs; s < ce; s++) {
-                if (s == (uint32_t)a.window) continue;
+                if (s == w) continue;
+                {   // L2 prefetch of the rows of the pair kPrefetchPairs ahead: its
+                    // context row (lane 0) and, inside this slot chunk, its negatives'
+                    // rows (lanes 1..neg); past this centre, the next centre's context row.
+                    const uint32_t kp = s - s_lo - (s > w ? 1u : 0u) + kPrefetchPairs;
+                    if (kp < n_pairs_here) {
+                        const uint32_t sp = s_lo + kp + (s_lo + kp >= w ? 1u : 0u);
+                        if (sp < ce) {
+                            if (lane == 0) prefetch_l2(a.syn0 + (size_t)sen[p - w + sp] * d, (uint32_t)d * 4);
+                            else if (lane <= (uint32_t)neg)
+                                prefetch_l2(a.syn1 + (size_t)tb[(sp - cs) * kFastNeg + lane - 1] * d, (uint32_t)d * 4);
+                        }
+                    } else if (p + 1 < n && lane == 0) {
+                        const uint32_t kq = kp - n_pairs_here;
+                        if (kq + 1 < q_hi - q_lo) {
+                            const uint32_t sq = q_lo + kq + (q_lo + kq >= w ? 1u : 0u);
+                            prefetch_l2(a.syn0 + (size_t)sen[p + 1 - w + sq] * d, (uint32_t)d * 4);
+                        }
+                    }
+                }
                 const int64_t c = (int64_t)p - a.window + s;
                 const int32_t last = sen[c];
                 float *l1p = a.syn0 + (size_t)last * d + lane * VEC;
-                int32_t t[kFastNeg];
+                int32_t t[NS];
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
+                for (int j = 0; j < NS; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
                 // Issue every row load of the pair before consuming any.
-                RowVec<VEC> l1, e, l2[kFastNeg];
+                RowVec<VEC> l1, e, l2[NS];
                 load_row<VEC>(l1p, l1);
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++)
+                for (int j = 0; j < NS; j++)
                     if (j < neg && t[j] != word) load_row<VEC>(a.syn1 + (size_t)t[j] * d + lane * VEC, l2[j]);
 #pragma unroll
                 for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
                 n_pairs++;
+                bool repeat = false;
+#pragma unroll
+                for (int j = 0; j < NS; j++)
+#pragma unroll
+                    for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
+                if (!repeat) {
+                    // No negative row occurs twice in the pair, so no target's dot
+                    // product reads another target's update: all 1 + neg dot products
+                    // (same per-lane order and tree as warp_dot) and their gradients
+                    // are formed together, one gradient per lane group, then
+                    // applied in the sequential order.
+                    constexpr int M = pow2_at_least(NS + 1);
+                    constexpr int GROUP = 32 / M;   // lanes holding one sum
+                    float f[M], g[NS + 1];
+                    {
+                        float s0 = 0.f;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
+                        f[0] = s0;
+                    }
+                    uint32_t live = 0;   // bit j: negative j has a row
+#pragma unroll
+                    for (int j = 0; j < NS; j++) {
+                        float sj = 0.f;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], l2[j].v[i], sj);
+                        f[j + 1] = sj;
+                        if (j < neg && t[j] != word) live |= 1u << j;
+                    }
+#pragma unroll
+                    for (int j = NS + 1; j < M; j++) f[j] = 0.f;
+                    const float mine = warp_sums_split<M>(f, lane);
+                    const uint32_t jm = lane / GROUP;
+                    // Slots without a row (and padding) get no table lookup.
+                    float gm = 0.f;
+                    if (jm == 0) gm = sg_grad(mine, 1, a.exp_table, alpha);
+                    else if (jm <= (uint32_t)NS && ((live >> (jm - 1)) & 1u)) gm = sg_grad(mine, 0, a.exp_table, alpha);
+#pragma unroll
+                    for (int j = 0; j <= NS; j++) g[j] = __shfl_sync(0xffffffffu, gm, j * GROUP);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < NS; j++) {
+                        if (!((live >> j) & 1u)) continue;
+                        RowVec<VEC> upd;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) {
+                            e.v[i] = fmaf(g[j + 1], l2[j].v[i], e.v[i]);
+                            upd.v[i] = __fmul_rn(g[j + 1], l1.v[i]);  // rounded product, never fused
+                        }
+                        float *l2p = a.syn1 + (size_t)t[j] * d + lane * VEC;
+                        if (a.deterministic) {
+#pragma unroll
+                            for (int i = 0; i < VEC; i++) l2[j].v[i] += upd.v[i];
+                            store_row<VEC>(l2p, l2[j]);
+                        } else {
+                            add_row<VEC>(l2p, upd);
+                        }
+                    }
+                } else {
                 {   // positive target: the centre word (kept in registers for this centre)
                     const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
 #pragma unroll
@@ -338,7 +476,7 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) {
+                for (int j = 0; j < NS; j++) {
                     if (j >= neg || t[j] == word) continue;
                     const float g = sg_grad(warp_dot<VEC>(l1, l2[j]), 0, a.exp_table, alpha);
                     RowVec<VEC> upd;
@@ -353,8 +491,9 @@ __global__ void __launch_bounds__(THREADS) sgns_plain_kernel(SgnsArgs a, WalkSet
                     else add_row<VEC>(l2p, upd);
                     // A later negative of this pair on the same row sees this update.
 #pragma unroll
-                    for (int k = j + 1; k < kFastNeg; k++)
+                    for (int k = j + 1; k < NS; k++)
                         if (t[k] == t[j]) l2[k] = l2[j];
+                }
                 }
                 if (a.deterministic) {
 #pragma unroll
@@ -484,8 +623,8 @@ struct BfRows {
 // rows: the same pairs, draws and update order as sgns_plain_kernel, arithmetic
 // in FP32; each row write rounds stochastically with noise keyed by
 // (row, walk, centre, slot), so a deterministic run is reproducible.
-template <int VEC, int THREADS>
-__global__ void __launch_bounds__(THREADS) sgns_plain_bf16_kernel(SgnsArgs a, WalkSet ws) {
+template <int VEC, int THREADS, int FIT>
+__global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
     __shared__ int32_t tb_all[THREADS / 32][kSlotChunk * kFastNeg];
     const uint32_t lane = threadIdx.x & 31;
@@ -803,15 +942,21 @@ static int plain_blocks(const dg_sgns *s, int resident, int threads) {
 }
 
 // One launch of the fast plain kernel in launch shape I (threads per block,
-// blocks per SM); dg_sgns_autotune picks the shape.
+// blocks per SM, register cap); dg_sgns_autotune picks the shape.
 template <int V, int I, bool BF>
 static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     constexpr int T = kPlainShapes[I].threads;
+    constexpr int FIT = V >= 8 ? 0 : kPlainShapes[I].fit;
     int blocks = 1, threads = 32;
     void (*kern)(SgnsArgs, WalkSet);
-    if constexpr (BF) kern = sgns_plain_bf16_kernel<V, T>;
-    else kern = sgns_plain_kernel<V, T>;
+    if constexpr (BF) kern = sgns_plain_bf16_kernel<V, T, FIT>;
+    else if (a.negative == kPlainNeg && a.vocab_size > 1) kern = sgns_plain_kernel<V, T, kPlainNeg, FIT>;
+    else kern = sgns_plain_kernel<V, T, 0, FIT>;
     if (!s->p.deterministic) {
+        // Register-capped shapes hold more blocks than the default shared-memory
+        // carveout leaves room for (10 KB a block of 64 threads).
+        if (FIT) cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                      cudaSharedmemCarveoutMaxShared);
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
         per_sm = std::max(per_sm, 1);
@@ -824,13 +969,15 @@ static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) 
 
 template <int V, bool BF>
 static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    static_assert(kPlainShapeCount == 5, "dispatch below lists every shape");
+    static_assert(kPlainShapeCount == 7, "dispatch below lists every shape");
     switch (s->plain_shape) {
     case 0: plain_fast_launch<V, 0, BF>(s, a, ws); break;
     case 1: plain_fast_launch<V, 1, BF>(s, a, ws); break;
     case 2: plain_fast_launch<V, 2, BF>(s, a, ws); break;
     case 3: plain_fast_launch<V, 3, BF>(s, a, ws); break;
     case 4: plain_fast_launch<V, 4, BF>(s, a, ws); break;
+    case 5: plain_fast_launch<V, 5, BF>(s, a, ws); break;
+    case 6: plain_fast_launch<V, 6, BF>(s, a, ws); break;
     default: return dg::fail(DG_ERR_ARG, "plain launch shape %d out of range", s->plain_shape);
     }
     return DG_OK;
@@ -1136,7 +1283,7 @@ extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info 
         if (k < DG_TUNE_MAX) {
             r.ms[k] = ms;
             r.shape[k][0] = dgs::kPlainShapes[k].threads;
-            r.shape[k][1] = dgs::kPlainShapes[k].per_sm;
+            r.shape[k][1] = dgs::kPlainShapes[k].per_sm ? dgs::kPlainShapes[k].per_sm : dgs::kPlainShapes[k].fit;
         }
         if (ms < best) {
             best = ms;

@@ -16,12 +16,16 @@ constexpr int kMaxExp = 6;                        // word2vec.cu:30
 constexpr uint64_t kDefaultTableSize = 100000000; // word2vec.cu:66
 constexpr uint32_t kMaxSentence = 1024;           // tokens of one walk used for training
 constexpr int kPlainThreads = 256;
-// Launch shapes of the fast plain kernel: threads per block (one walk per warp)
-// and blocks per SM (0: as many as fit).  Shape 0 is the default.
+// Launch shapes of the fast plain kernel: threads per block (one walk per warp),
+// blocks per SM (0: as many as fit) and, for register-capped instances, the
+// number of resident blocks per SM the kernel is compiled to fit (its
+// __launch_bounds__ minimum; 0: no cap; ignored for rows of 256 floats and
+// more, where the cap would spill).  Shape 0 is the default.
 struct PlainShape {
-    int threads, per_sm;
+    int threads, per_sm, fit;
 };
-constexpr PlainShape kPlainShapes[] = {{256, 0}, {128, 0}, {64, 0}, {256, 2}, {128, 4}};
+constexpr PlainShape kPlainShapes[] = {{256, 0, 0}, {128, 0, 0}, {64, 0, 0}, {64, 0, 12},
+                                       {64, 0, 16}, {256, 2, 0}, {128, 4, 0}};
 constexpr int kPlainShapeCount = (int)(sizeof(kPlainShapes) / sizeof(kPlainShapes[0]));
 constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
 

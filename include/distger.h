@@ -283,7 +283,9 @@ typedef struct {
     int n_candidates;
     int chosen;                /* index of the shape kept */
     int shape[DG_TUNE_MAX][2]; /* walks: {walks per block, footprints cached in shared memory per walk};
-                                  plain SGNS: {threads per block, blocks per SM (0 = as many as fit)} */
+                                  plain SGNS: {threads per block, blocks per SM: 0 = as many as fit,
+                                  else that many (a cap, or the count the kernel's registers
+                                  are limited to fit)} */
     double ms[DG_TUNE_MAX];    /* kernel time of each candidate (CUDA events) */
 } dg_tune_info;
 

@@ -418,12 +418,12 @@ def run_auc_ours(args, local):
         clocks = Clocks(local)
         clocks.start()
         res = embed(graph, mode=mode, seed=args.seed, workers=workers, deterministic=2 if variant == "adjoint" else 0,
-                    master_rows=args.master_rows, device=local, **AUC_HP)
+                    master_rows=args.master_rows, device=local, plain_shape=args.plain_shape, **AUC_HP)
         clk = clocks.stop()
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16",
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "f32" if mode == "plain" else "bf16",
                           "workers": workers or res["workers"], "master_rows": args.master_rows, "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
@@ -512,14 +512,14 @@ def run_auc_synth(args, local):
         clocks.start()
         res = embed(graph, mode=mode, seed=args.seed, rounds=args.rounds, init_round=cfg["min_r"], max_len=32,
                     deterministic=2 if variant == "adjoint" else 0, workers=workers, master_rows=args.master_rows,
-                    keep_trainer=True, device=local, **AUC_HP)
+                    keep_trainer=True, device=local, plain_shape=args.plain_shape, **AUC_HP)
         clk = clocks.stop()
         t4 = time.perf_counter()
         sgns = res.pop("trainer")
         m = pairs.auc(sgns)
         t5 = time.perf_counter()
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "dtype": "f32" if mode == "plain" else "bf16", "workers": res["workers"],
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "f32" if mode == "plain" else "bf16", "workers": res["workers"],
                           "master_rows": args.master_rows,
                           "auc": m["auc"], "auc_cosine": m["auc_cosine"], "test_pairs": pairs.n_pos + pairs.n_neg,
                           "vertices": cfg["n"], "undirected_edges": n_edges, "rounds": len(res["rounds"]),
@@ -590,6 +590,8 @@ def main():
                     help="graph of the --auc run (c5_twitter and *_device: generated and split on the device)")
     ap.add_argument("--rounds", type=int, default=30, help="--auc on device-generated graphs: walk rounds")
     ap.add_argument("--auc-modes", default="plain,minibatch")
+    ap.add_argument("--plain-shape", type=int, default=None,
+                    help="AUC runs: launch shape of the plain kernel (an index of the autotuner's list)")
     ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--master-rows", type=int, default=0, help="--auc: FP32 master rows of the minibatch form")

@@ -237,13 +237,15 @@ __device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, u
 
 // Builds the walk's sentence in shared memory: vocabulary lookup + subsampling
 // (word2vec.cu:1011-1029 with a Philox draw in place of rand()).  Returns its length.
+// At most CAP tokens of a walk are used.
+template <uint32_t CAP = kMaxSentence>
 __device__ __forceinline__ uint32_t warp_sentence(const WalkSet &ws, uint32_t walk, const SgnsArgs &a, int32_t *sen,
                                                   uint32_t &words) {
     const uint32_t lane = threadIdx.x & 31;
     uint64_t begin;
     uint32_t len;
     ws.range(walk, begin, len);
-    if (len > kMaxSentence) len = kMaxSentence;
+    if (len > CAP) len = CAP;
     words = len;
     uint32_t n = 0;
     for (uint32_t base = 0; base < len; base += 32) {
@@ -292,8 +294,9 @@ constexpr uint32_t kSlotChunk = 32;   // window slots whose negatives are drawn 
 // slot), all lanes at once, so that the pairs of a centre wait on the unigram
 // table once instead of once per pair.  The draws are the per-pair draws
 // (negative_target), so the result is unchanged.  Slot == window is skipped.
+// Slot cs + k, negative j goes to tb[k * stride + j].
 __device__ __forceinline__ void draw_negatives(const SgnsArgs &a, uint32_t p, uint32_t wid, uint32_t cs, uint32_t ce,
-                                               int neg, int32_t *tb) {
+                                               int neg, int32_t *tb, int stride = kFastNeg) {
     const uint32_t lane = threadIdx.x & 31;
     __syncwarp();
     const uint32_t total = (ce - cs) * (uint32_t)neg;
@@ -301,7 +304,7 @@ __device__ __forceinline__ void draw_negatives(const SgnsArgs &a, uint32_t p, ui
         const uint32_t k = q / (uint32_t)neg, j = q % (uint32_t)neg;
         const uint32_t s = cs + k;
         if (s == (uint32_t)a.window) continue;
-        tb[k * kFastNeg + j] = negative_target(a, p, s, wid, (int)j + 1);
+        tb[k * stride + j] = negative_target(a, p, s, wid, (int)j + 1);
     }
     __syncwarp();
 }
@@ -520,6 +523,292 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(
     }
 }
 
+// ------------------------------------------ plain rule, rows staged ahead
+
+// Hogwild form of the plain rule whose row loads overlap the previous pairs'
+// arithmetic: while pair m computes, the rows of pair m + S - 1 (its context row
+// and its negatives' rows) are copied into this warp's shared memory with
+// cp.async, so a pair waits on a copy issued S - 1 pairs earlier instead of a
+// DRAM round trip.  Each lane copies, and later reads, only its own columns.
+// A copy made before this warp's last updates of the same row would miss them;
+// the kernel restores them where they matter:
+//  * context rows: a context word used by one of the previous S pairs is read
+//    from that pair's updated row (kept in shared memory), so a context row sees
+//    every update of this warp, as in sgns_plain_kernel;
+//  * the centre's output row is loaded when the centre starts (after every
+//    earlier update) and kept in registers, as in sgns_plain_kernel;
+//  * a negative's output row copied before one of the previous S pairs (or a
+//    finished centre) updated it misses that update: staleness of at most S
+//    pairs, of the kind other warps' concurrent updates cause in any Hogwild run.
+// Draws, pairs, sums, gradients and the update order of each pair are
+// sgns_plain_kernel's.  The launcher uses it only without `deterministic`, for
+// sentences of at most kPipeSentence tokens, window <= kPipeMaxWindow and
+// negative <= kFastNeg.
+constexpr uint32_t kPipeSentence = 64;
+constexpr int kPipeMaxWindow = 15;
+
+template <int VEC>
+__device__ __forceinline__ void copy_row_async(float *dst, const float *src) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst);
+    const size_t ga = __cvta_generic_to_global(src);
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa + 4 * i), "l"(ga + 4 * i) : "memory");
+    } else if constexpr (VEC == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(ga) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(ga) : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// This lane's columns of a row held in shared memory.
+template <int VEC>
+__device__ __forceinline__ void lds_row(const float *p, RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4) {
+            const float4 t = *reinterpret_cast<const float4 *>(p + i);
+            r.v[i] = t.x; r.v[i + 1] = t.y; r.v[i + 2] = t.z; r.v[i + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) r.v[i] = p[i];
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void sts_row(float *p, const RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            *reinterpret_cast<float4 *>(p + i) = make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) p[i] = r.v[i];
+    }
+}
+
+template <int VEC, int NS, int S>
+struct alignas(16) PipeWarp {
+    float stage[S][1 + NS][32 * VEC];             // rows of S pairs: context, negatives 0..NS-1
+    float hist[S][32 * VEC];                      // updated context rows of the last S pairs
+    int32_t sen[kPipeSentence];
+    int32_t tb[S][(2 * kPipeMaxWindow + 1) * NS];  // negatives of S centres, ring by centre
+    uint16_t lohi[kPipeSentence];                 // slot range of each centre: lo | hi << 8
+};
+
+template <int VEC, int THREADS, int NEG, int S, int FIT>
+__global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_kernel(SgnsArgs a, WalkSet ws) {
+    constexpr int NS = NEG > 0 ? NEG : kFastNeg;
+    constexpr int D = 32 * VEC;
+    constexpr int M = pow2_at_least(NS + 1);
+    constexpr int GROUP = 32 / M;
+    __shared__ PipeWarp<VEC, NS, S> sm_all[THREADS / 32];
+    PipeWarp<VEC, NS, S> &sm = sm_all[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t w = (uint32_t)a.window;
+    const float alpha = a.alpha;
+    const int neg = NEG > 0 ? NEG : (a.vocab_size > 1 ? a.negative : 0);
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    int32_t hw[S];   // context words of this warp's last S pairs, newest first
+#pragma unroll
+    for (int k = 0; k < S; k++) hw[k] = -1;
+    uint32_t mm = 0;  // pairs trained by this warp (ring position of hist)
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence<kPipeSentence>(ws, walk, a, sm.sen, words);
+        n_words += words;
+        n_trained += n;
+        if (n < 2) continue;   // a one-token sentence has no pairs
+        for (uint32_t q = lane; q < n; q += 32) {
+            const uint32_t b = philox(q, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
+            uint32_t lo, hi;
+            slot_range(q, n, w, b, lo, hi);
+            sm.lohi[q] = (uint16_t)(lo | (hi << 8));
+        }
+        __syncwarp();
+        // With n >= 2 every centre has a pair, and slot w lies inside its range.
+        auto first_slot = [&](uint32_t q) {
+            const uint32_t s0 = sm.lohi[q] & 0xFFu;
+            return s0 == w ? s0 + 1 : s0;
+        };
+        auto advance = [&](uint32_t &q, uint32_t &s) {   // next pair; true when centre q ended
+            s++;
+            if (s == w) s++;
+            if (s < (uint32_t)(sm.lohi[q] >> 8)) return false;
+            q++;
+            if (q < n) s = first_slot(q);
+            return true;
+        };
+        auto enter = [&](uint32_t q) {   // the copies reach centre q: draw its negatives
+            const uint32_t lo = sm.lohi[q] & 0xFFu, hi = sm.lohi[q] >> 8;
+            draw_negatives(a, q, wid, lo, hi, neg, sm.tb[q % S], NS);
+            if (lane == 0) prefetch_l2(a.syn1 + (size_t)sm.sen[q] * D, (uint32_t)D * 4);
+        };
+        auto issue = [&](uint32_t q, uint32_t s, uint32_t st) {
+            const int32_t ctx = sm.sen[q - w + s];
+            copy_row_async<VEC>(&sm.stage[st][0][lane * VEC], a.syn0 + (size_t)ctx * D + lane * VEC);
+            const int32_t *tq = sm.tb[q % S] + (s - (sm.lohi[q] & 0xFFu)) * NS;
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+                if (j < neg)
+                    copy_row_async<VEC>(&sm.stage[st][1 + j][lane * VEC], a.syn1 + (size_t)tq[j] * D + lane * VEC);
+        };
+        uint32_t pp = 0, sp = first_slot(0);   // next pair to copy
+        enter(0);
+#pragma unroll
+        for (int i = 0; i < S - 1; i++) {
+            if (pp < n) {
+                issue(pp, sp, (uint32_t)i);
+                if (advance(pp, sp) && pp < n) enter(pp);
+            }
+            cp_async_commit();
+        }
+        uint32_t p = 0, s = first_slot(0);     // pair to train
+        float *pos_row = a.syn1 + (size_t)sm.sen[0] * D + lane * VEC;
+        RowVec<VEC> pos, pos0;
+        load_row<VEC>(pos_row, pos);
+        pos0 = pos;
+        for (uint32_t m = 0; p < n; m++) {
+            if (pp < n) {
+                issue(pp, sp, (m + S - 1) % S);
+                if (advance(pp, sp) && pp < n) enter(pp);
+            }
+            cp_async_commit();
+            cp_async_wait<S - 1>();   // this lane's copies of pair m have landed
+            const uint32_t st = m % S;
+            const int32_t word = sm.sen[p];
+            const int32_t last = sm.sen[p - w + s];
+            RowVec<VEC> l1, e;
+            lds_row<VEC>(&sm.stage[st][0][lane * VEC], l1);
+#pragma unroll
+            for (int k = S - 1; k >= 0; k--)   // newest match last: it wins
+                if (hw[k] == last) lds_row<VEC>(&sm.hist[(mm + S - 1 - k) % S][lane * VEC], l1);
+            const int32_t *tq = sm.tb[p % S] + (s - (sm.lohi[p] & 0xFFu)) * NS;
+            int32_t t[NS];
+#pragma unroll
+            for (int j = 0; j < NS; j++) t[j] = j < neg ? tq[j] : -1;
+#pragma unroll
+            for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
+            n_pairs++;
+            bool repeat = false;
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+#pragma unroll
+                for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
+            if (!repeat) {   // as in sgns_plain_kernel: all sums and gradients at once
+                float f[M], g[NS + 1];
+                {
+                    float s0 = 0.f;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
+                    f[0] = s0;
+                }
+                uint32_t live = 0;
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    float sj = 0.f;
+                    if (j < neg) {
+                        RowVec<VEC> r;
+                        lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], r.v[i], sj);
+                        if (t[j] != word) live |= 1u << j;
+                    }
+                    f[j + 1] = sj;
+                }
+#pragma unroll
+                for (int j = NS + 1; j < M; j++) f[j] = 0.f;
+                const float mine = warp_sums_split<M>(f, lane);
+                const uint32_t jm = lane / GROUP;
+                float gm = 0.f;
+                if (jm == 0) gm = sg_grad(mine, 1, a.exp_table, alpha);
+                else if (jm <= (uint32_t)NS && ((live >> (jm - 1)) & 1u)) gm = sg_grad(mine, 0, a.exp_table, alpha);
+#pragma unroll
+                for (int j = 0; j <= NS; j++) g[j] = __shfl_sync(0xffffffffu, gm, j * GROUP);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) {
+                    e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
+                    pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                }
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    if (!((live >> j) & 1u)) continue;
+                    RowVec<VEC> r, upd;
+                    lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g[j + 1], r.v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g[j + 1], l1.v[i]);  // rounded product, never fused
+                    }
+                    add_row<VEC>(a.syn1 + (size_t)t[j] * D + lane * VEC, upd);
+                }
+            } else {   // a negative repeats: one target after the other
+                {
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    if (j >= neg || t[j] == word) continue;
+                    RowVec<VEC> r, upd;
+                    lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
+                    const float g = sg_grad(warp_dot<VEC>(l1, r), 0, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, r.v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, l1.v[i]);
+                        r.v[i] += upd.v[i];
+                    }
+                    add_row<VEC>(a.syn1 + (size_t)t[j] * D + lane * VEC, upd);
+                    // A later negative of this pair on the same row sees this update.
+#pragma unroll
+                    for (int k = j + 1; k < NS; k++)
+                        if (t[k] == t[j]) sts_row<VEC>(&sm.stage[st][1 + k][lane * VEC], r);
+                }
+            }
+            add_row<VEC>(a.syn0 + (size_t)last * D + lane * VEC, e);
+#pragma unroll
+            for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
+            sts_row<VEC>(&sm.hist[mm % S][lane * VEC], l1);
+#pragma unroll
+            for (int k = S - 1; k > 0; k--) hw[k] = hw[k - 1];
+            hw[0] = last;
+            mm++;
+            if (advance(p, s)) {   // centre done: its output row's update, then the next centre's row
+#pragma unroll
+                for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
+                add_row<VEC>(pos_row, pos);
+                if (p < n) {
+                    pos_row = a.syn1 + (size_t)sm.sen[p] * D + lane * VEC;
+                    load_row<VEC>(pos_row, pos);
+                    pos0 = pos;
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
 // ---------------------------------------------------- plain rule, BF16 rows
 
 __device__ __forceinline__ uint32_t bf_mix(uint32_t h) {
@@ -623,8 +912,10 @@ struct BfRows {
 // rows: the same pairs, draws and update order as sgns_plain_kernel, arithmetic
 // in FP32; each row write rounds stochastically with noise keyed by
 // (row, walk, centre, slot), so a deterministic run is reproducible.
-template <int VEC, int THREADS, int FIT>
+// NEG as in sgns_plain_kernel.
+template <int VEC, int THREADS, int NEG, int FIT>
 __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_kernel(SgnsArgs a, WalkSet ws) {
+    constexpr int NS = NEG > 0 ? NEG : kFastNeg;
     __shared__ int32_t sen_all[THREADS / 32][kMaxSentence];
     __shared__ int32_t tb_all[THREADS / 32][kSlotChunk * kFastNeg];
     const uint32_t lane = threadIdx.x & 31;
@@ -633,7 +924,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
     int32_t *tb = tb_all[warp];
     const int d = 32 * VEC;
     const float alpha = a.alpha;
-    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    const int neg = NEG > 0 ? NEG : (a.vocab_size > 1 ? a.negative : 0);
     const BfRows<VEC> in{a.in_bf, a.in_master, a.n_master, d};
     const BfRows<VEC> out{a.out_bf, a.out_master, a.n_master, d};
     const uint32_t key = a.seed_lo ^ bf_mix(a.pass * 0x9E3779B9u + 0x2F6B3A91u);
@@ -665,17 +956,70 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
                 if (s == (uint32_t)a.window) continue;
                 const int64_t c = (int64_t)p - a.window + s;
                 const int32_t last = sen[c];
-                int32_t t[kFastNeg];
+                int32_t t[NS];
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
-                RowVec<VEC> l1, e, l2[kFastNeg];
+                for (int j = 0; j < NS; j++) t[j] = j < neg ? tb[(s - cs) * kFastNeg + j] : -1;
+                RowVec<VEC> l1, e, l2[NS];
                 in.load(last, lane, l1);
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++)
+                for (int j = 0; j < NS; j++)
                     if (j < neg && t[j] != word) out.load(t[j], lane, l2[j]);
 #pragma unroll
                 for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
                 n_pairs++;
+                bool repeat = false;
+#pragma unroll
+                for (int j = 0; j < NS; j++)
+#pragma unroll
+                    for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
+                if (!repeat) {   // all sums and gradients at once, as in sgns_plain_kernel
+                    constexpr int M = pow2_at_least(NS + 1);
+                    constexpr int GROUP = 32 / M;
+                    float f[M], g[NS + 1];
+                    {
+                        float s0 = 0.f;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
+                        f[0] = s0;
+                    }
+                    uint32_t live = 0;
+#pragma unroll
+                    for (int j = 0; j < NS; j++) {
+                        float sj = 0.f;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], l2[j].v[i], sj);
+                        f[j + 1] = sj;
+                        if (j < neg && t[j] != word) live |= 1u << j;
+                    }
+#pragma unroll
+                    for (int j = NS + 1; j < M; j++) f[j] = 0.f;
+                    const float mine = warp_sums_split<M>(f, lane);
+                    const uint32_t jm = lane / GROUP;
+                    float gm = 0.f;
+                    if (jm == 0) gm = sg_grad(mine, 1, a.exp_table, alpha);
+                    else if (jm <= (uint32_t)NS && ((live >> (jm - 1)) & 1u)) gm = sg_grad(mine, 0, a.exp_table, alpha);
+#pragma unroll
+                    for (int j = 0; j <= NS; j++) g[j] = __shfl_sync(0xffffffffu, gm, j * GROUP);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                    }
+#pragma unroll
+                    for (int j = 0; j < NS; j++) {
+                        if (!((live >> j) & 1u)) continue;
+                        RowVec<VEC> upd;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) {
+                            e.v[i] = fmaf(g[j + 1], l2[j].v[i], e.v[i]);
+                            upd.v[i] = __fmul_rn(g[j + 1], l1.v[i]);
+                            l2[j].v[i] += upd.v[i];
+                        }
+                        const uint32_t salt = base + (uint32_t)t[j] * 0x27D4EB2Fu + s * 16u + (uint32_t)j;
+                        if (a.deterministic) out.put(t[j], lane, l2[j], salt);
+                        else out.update(t[j], lane, upd, l2[j], salt);
+                    }
+                } else {
                 {
                     const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
 #pragma unroll
@@ -685,7 +1029,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
                     }
                 }
 #pragma unroll
-                for (int j = 0; j < kFastNeg; j++) {
+                for (int j = 0; j < NS; j++) {
                     if (j >= neg || t[j] == word) continue;
                     const float g = sg_grad(warp_dot<VEC>(l1, l2[j]), 0, a.exp_table, alpha);
                     RowVec<VEC> upd;
@@ -699,8 +1043,9 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
                     if (a.deterministic) out.put(t[j], lane, l2[j], salt);
                     else out.update(t[j], lane, upd, l2[j], salt);
 #pragma unroll
-                    for (int k = j + 1; k < kFastNeg; k++)
+                    for (int k = j + 1; k < NS; k++)
                         if (t[k] == t[j]) l2[k] = l2[j];
+                }
                 }
                 const uint32_t salt1 = base + (uint32_t)last * 0x165667B1u + s * 16u + 15u;
 #pragma unroll
@@ -943,20 +1288,38 @@ static int plain_blocks(const dg_sgns *s, int resident, int threads) {
 
 // One launch of the fast plain kernel in launch shape I (threads per block,
 // blocks per SM, register cap); dg_sgns_autotune picks the shape.
+// The staged-rows kernel's conditions (see sgns_plain_pipe_kernel).
+static bool pipe_applies(const dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    return !s->p.deterministic && ws.max_len > 0 && ws.max_len <= kPipeSentence && a.window <= kPipeMaxWindow &&
+           a.negative <= kFastNeg;
+}
+
 template <int V, int I, bool BF>
 static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     constexpr int T = kPlainShapes[I].threads;
     constexpr int FIT = V >= 8 ? 0 : kPlainShapes[I].fit;
+    constexpr int STG = kPlainShapes[I].stages;
     int blocks = 1, threads = 32;
     void (*kern)(SgnsArgs, WalkSet);
-    if constexpr (BF) kern = sgns_plain_bf16_kernel<V, T, FIT>;
-    else if (a.negative == kPlainNeg && a.vocab_size > 1) kern = sgns_plain_kernel<V, T, kPlainNeg, FIT>;
-    else kern = sgns_plain_kernel<V, T, 0, FIT>;
+    bool staged = false;
+    const bool neg_fixed = a.negative == kPlainNeg && a.vocab_size > 1;
+    if constexpr (BF) {
+        kern = neg_fixed ? sgns_plain_bf16_kernel<V, T, kPlainNeg, FIT> : sgns_plain_bf16_kernel<V, T, 0, FIT>;
+    } else {
+        kern = neg_fixed ? sgns_plain_kernel<V, T, kPlainNeg, FIT> : sgns_plain_kernel<V, T, 0, FIT>;
+        if constexpr (STG >= 2 && (V == 2 || V == 4)) {
+            if (pipe_applies(s, a, ws)) {
+                kern = neg_fixed ? sgns_plain_pipe_kernel<V, T, kPlainNeg, STG, FIT>
+                                 : sgns_plain_pipe_kernel<V, T, 0, STG, FIT>;
+                staged = true;
+            }
+        }
+    }
     if (!s->p.deterministic) {
-        // Register-capped shapes hold more blocks than the default shared-memory
-        // carveout leaves room for (10 KB a block of 64 threads).
-        if (FIT) cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout,
-                                      cudaSharedmemCarveoutMaxShared);
+        // Register-capped shapes and the staged-rows kernel hold more blocks than
+        // the default shared-memory carveout leaves room for.
+        if (FIT || staged)
+            cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, cudaSharedmemCarveoutMaxShared);
         int per_sm = 0;
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, T, 0);
         per_sm = std::max(per_sm, 1);
@@ -969,7 +1332,7 @@ static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) 
 
 template <int V, bool BF>
 static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    static_assert(kPlainShapeCount == 7, "dispatch below lists every shape");
+    static_assert(kPlainShapeCount == 12, "dispatch below lists every shape");
     switch (s->plain_shape) {
     case 0: plain_fast_launch<V, 0, BF>(s, a, ws); break;
     case 1: plain_fast_launch<V, 1, BF>(s, a, ws); break;
@@ -978,6 +1341,11 @@ static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     case 4: plain_fast_launch<V, 4, BF>(s, a, ws); break;
     case 5: plain_fast_launch<V, 5, BF>(s, a, ws); break;
     case 6: plain_fast_launch<V, 6, BF>(s, a, ws); break;
+    case 7: plain_fast_launch<V, 7, BF>(s, a, ws); break;
+    case 8: plain_fast_launch<V, 8, BF>(s, a, ws); break;
+    case 9: plain_fast_launch<V, 9, BF>(s, a, ws); break;
+    case 10: plain_fast_launch<V, 10, BF>(s, a, ws); break;
+    case 11: plain_fast_launch<V, 11, BF>(s, a, ws); break;
     default: return dg::fail(DG_ERR_ARG, "plain launch shape %d out of range", s->plain_shape);
     }
     return DG_OK;
@@ -1284,6 +1652,7 @@ extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info 
             r.ms[k] = ms;
             r.shape[k][0] = dgs::kPlainShapes[k].threads;
             r.shape[k][1] = dgs::kPlainShapes[k].per_sm ? dgs::kPlainShapes[k].per_sm : dgs::kPlainShapes[k].fit;
+            r.shape[k][2] = dgs::kPlainShapes[k].stages;
         }
         if (ms < best) {
             best = ms;
@@ -1314,6 +1683,7 @@ extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alph
     ws.lens = paths->lens.p;
     ws.stride = paths->stride;
     ws.n_walks = paths->n_walks;
+    ws.max_len = paths->info.max_len;
     ws.id_base = 0;
     // The walk stream and the trainer stream are ordered by synchronising here.
     dg::DeviceGuard guard(s->device);
@@ -1375,6 +1745,8 @@ extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t 
     ws.verts = d_verts.p;
     ws.offsets = d_off.p;
     ws.n_walks = n_walks;
+    for (uint32_t i = 0; i < n_walks; i++)
+        ws.max_len = (uint32_t)std::max<uint64_t>(ws.max_len, std::min<uint64_t>(offsets[i + 1] - offsets[i], UINT32_MAX));
     ws.id_base = 0;
     return train_walks(s, ws, alpha, info);
 }

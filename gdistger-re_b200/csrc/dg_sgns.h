@@ -17,15 +17,18 @@ constexpr uint64_t kDefaultTableSize = 100000000; // word2vec.cu:66
 constexpr uint32_t kMaxSentence = 1024;           // tokens of one walk used for training
 constexpr int kPlainThreads = 256;
 // Launch shapes of the fast plain kernel: threads per block (one walk per warp),
-// blocks per SM (0: as many as fit) and, for register-capped instances, the
-// number of resident blocks per SM the kernel is compiled to fit (its
-// __launch_bounds__ minimum; 0: no cap; ignored for rows of 256 floats and
-// more, where the cap would spill).  Shape 0 is the default.
+// blocks per SM (0: as many as fit), for register-capped instances the number
+// of resident blocks per SM the kernel is compiled to fit (its __launch_bounds__
+// minimum; 0: no cap; ignored for rows of 256 floats and more, where the cap
+// would spill), and the pairs whose rows are staged ahead in shared memory
+// (0: sgns_plain_kernel; S >= 2: sgns_plain_pipe_kernel where it applies, else
+// sgns_plain_kernel with the same threads and cap).  Shape 0 is the default.
 struct PlainShape {
-    int threads, per_sm, fit;
+    int threads, per_sm, fit, stages;
 };
-constexpr PlainShape kPlainShapes[] = {{256, 0, 0}, {128, 0, 0}, {64, 0, 0}, {64, 0, 12},
-                                       {64, 0, 16}, {256, 2, 0}, {128, 4, 0}};
+constexpr PlainShape kPlainShapes[] = {{256, 0, 0, 0}, {128, 0, 0, 0}, {64, 0, 0, 0},  {64, 0, 12, 0},
+                                       {64, 0, 16, 0}, {256, 2, 0, 0}, {128, 4, 0, 0}, {64, 0, 0, 2},
+                                       {64, 0, 12, 2}, {64, 0, 16, 2}, {64, 0, 12, 3}, {64, 0, 0, 3}};
 constexpr int kPlainShapeCount = (int)(sizeof(kPlainShapes) / sizeof(kPlainShapes[0]));
 constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
 
@@ -43,6 +46,7 @@ struct WalkSet {
     const uint32_t *ids = nullptr;  // walk id for the random counters (default: index + id_base)
     uint32_t stride = 0;
     uint32_t n_walks = 0;
+    uint32_t max_len = 0;            // longest walk in footprints (0: not known)
     uint32_t id_base = 0;
     __device__ __forceinline__ void range(uint32_t w, uint64_t &begin, uint32_t &len) const {
         if (offsets) {

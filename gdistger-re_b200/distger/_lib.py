@@ -81,12 +81,12 @@ class SgnsPairs(C.Structure):
 
 class TuneInfo(C.Structure):
     """dg_tune_info: the launch shapes timed by an autotune call and the one kept."""
-    _fields_ = [("n_candidates", C.c_int), ("chosen", C.c_int), ("shape", (C.c_int * 2) * 8),
-                ("ms", C.c_double * 8)]
+    _fields_ = [("n_candidates", C.c_int), ("chosen", C.c_int), ("shape", (C.c_int * 3) * 16),
+                ("ms", C.c_double * 16)]
 
     def as_dict(self) -> dict:
-        n = min(self.n_candidates, 8)
-        return {"chosen": self.chosen, "candidates": [{"shape": [self.shape[k][0], self.shape[k][1]],
+        n = min(self.n_candidates, 16)
+        return {"chosen": self.chosen, "candidates": [{"shape": [self.shape[k][0], self.shape[k][1], self.shape[k][2]],
                                                        "ms": self.ms[k]} for k in range(n)]}
 
 

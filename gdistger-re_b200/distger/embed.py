@@ -37,9 +37,10 @@ def embed(graph: Graph, walker_num: int | None = None, mode: str = "plain", size
           negative: int = 5, batch_size: int = 21, sample: float = 1e-3, alpha: float = 0.01, iter: int = 1,
           min_count: int = 0, rounds: int = LAST_ROUND, init_round: int = 5, min_len: int = 20, lr: str = "exp",
           train_from: int = 1, seed: int = 1, master_rows: int = 0, workers: int = 0, deterministic: int = 0,
-          max_len: int = 64, keep_trainer: bool = False, device: int = 0) -> dict:
+          max_len: int = 64, keep_trainer: bool = False, device: int = 0, plain_shape: int | None = None) -> dict:
     """Runs the job on `graph` and returns the embedding in vertex order plus the job's counters.
-    deterministic = 2 trains by adjoint gradient steps (see dg_sgns_params)."""
+    deterministic = 2 trains by adjoint gradient steps (see dg_sgns_params); plain_shape
+    selects a launch shape of the plain kernel (SGNS.set_shape)."""
     t0 = time.perf_counter()
     v_num = graph.v_num
     walker_num = walker_num or v_num
@@ -48,6 +49,8 @@ def embed(graph: Graph, walker_num: int | None = None, mode: str = "plain", size
     sgns = SGNS(v_num, counts, size=size, window=window, negative=negative, batch_size=batch_size, sample=sample,
                 alpha=alpha, iter=iter, min_count=min_count, mode=mode, seed=seed, master_rows=master_rows,
                 workers=workers, deterministic=deterministic, device=device)
+    if plain_shape is not None:
+        sgns.set_shape(plain_shape)
     wp = _lib.WalkParams(min_len=min_len, init_round=init_round, walker_num=walker_num, max_len=max_len, seed=seed)
     sched = make_lr(lr, alpha, rounds)
     L = lib()

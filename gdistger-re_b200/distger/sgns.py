@@ -58,6 +58,11 @@ class SGNS:
         check(lib().dg_sgns_autotune(self._h, paths.handle, C.byref(info)))
         return info.as_dict()
 
+    def set_shape(self, shape: int) -> None:
+        """Selects launch shape `shape` of the plain kernel (an index of the list
+        autotune times)."""
+        check(lib().dg_sgns_set_shape(self._h, int(shape)))
+
     def train_paths(self, paths, alpha: float = 0.0) -> _lib.TrainInfo:
         info = _lib.TrainInfo()
         check(lib().dg_sgns_train_paths(self._h, paths.handle, alpha, C.byref(info)))

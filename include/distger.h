@@ -278,14 +278,15 @@ DG_API int dg_lp_auc(const dg_sgns *s, const dg_lp_pairs *t, double *auc, double
  * for later calls.  Results never depend on the shape: walks are keyed by
  * walker id, and the plain trainer's Hogwild updates depend on scheduling
  * under every shape alike. */
-#define DG_TUNE_MAX 8
+#define DG_TUNE_MAX 16
 typedef struct {
     int n_candidates;
     int chosen;                /* index of the shape kept */
-    int shape[DG_TUNE_MAX][2]; /* walks: {walks per block, footprints cached in shared memory per walk};
+    int shape[DG_TUNE_MAX][3]; /* walks: {walks per block, footprints cached in shared memory per walk, 0};
                                   plain SGNS: {threads per block, blocks per SM: 0 = as many as fit,
                                   else that many (a cap, or the count the kernel's registers
-                                  are limited to fit)} */
+                                  are limited to fit), pairs whose rows are staged in shared
+                                  memory (0: rows loaded when the pair starts)} */
     double ms[DG_TUNE_MAX];    /* kernel time of each candidate (CUDA events) */
 } dg_tune_info;
 

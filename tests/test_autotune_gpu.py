@@ -60,7 +60,7 @@ def test_sgns_autotune_restores_rows(distger_lib, c1):
     s.train_paths(p)
     rows0, out0 = s.embedding()[0], s.output_rows()
     info = s.autotune(p)
-    assert len(info["candidates"]) == 7 and 0 <= info["chosen"] < 7
+    assert len(info["candidates"]) == 12 and 0 <= info["chosen"] < 12
     assert np.array_equal(s.embedding()[0].view(np.uint32), rows0.view(np.uint32))
     assert np.array_equal(s.output_rows().view(np.uint32), out0.view(np.uint32))
     t = s.train_paths(p)

@@ -26,9 +26,9 @@ constexpr int kPlainThreads = 256;
 struct PlainShape {
     int threads, per_sm, fit, stages;
 };
-constexpr PlainShape kPlainShapes[] = {{256, 0, 0, 0}, {128, 0, 0, 0}, {64, 0, 0, 0},  {64, 0, 12, 0},
-                                       {64, 0, 16, 0}, {256, 2, 0, 0}, {128, 4, 0, 0}, {64, 0, 0, 2},
-                                       {64, 0, 12, 2}, {64, 0, 16, 2}, {64, 0, 12, 3}, {64, 0, 0, 3}};
+constexpr PlainShape kPlainShapes[] = {{64, 0, 12, 2}, {256, 0, 0, 0}, {128, 0, 0, 0}, {64, 0, 0, 0},
+                                       {64, 0, 12, 0}, {64, 0, 16, 0}, {256, 2, 0, 0}, {128, 4, 0, 0},
+                                       {64, 0, 0, 2},  {64, 0, 16, 2}, {64, 0, 12, 3}, {64, 0, 0, 3}};
 constexpr int kPlainShapeCount = (int)(sizeof(kPlainShapes) / sizeof(kPlainShapes[0]));
 constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
 

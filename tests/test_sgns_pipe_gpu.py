@@ -14,7 +14,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-UNSTAGED, STAGED2, STAGED3 = 3, 8, 10   # launch shapes {64, 0, 12, 0}, {64, 0, 12, 2}, {64, 0, 12, 3}
+UNSTAGED, STAGED2, STAGED3 = 4, 0, 10   # launch shapes {64, 0, 12, 0}, {64, 0, 12, 2}, {64, 0, 12, 3}
 
 
 @pytest.fixture(scope="module")

@@ -125,6 +125,13 @@ struct dg_graph {
     uint64_t visits_total = 0;        // footprints over all rounds (sum of freq)
     double threshold_ms = 0.0;
     int walk_shape = 0;               // walk_kernel launch shape (dg_walk_autotune)
+    // Per-round buffers kept between rounds, so a round allocates nothing once
+    // the first has run: counters, the visit counts' backup, entropy partial
+    // sums, and the walk arena of the last freed dg_paths (largest kept).
+    dg::DevArray<unsigned long long> round_stats;
+    dg::DevArray<uint32_t> round_ctl, freq_backup;
+    dg::DevArray<double> entropy_partial;
+    dg::DevArray<uint32_t> spare_verts, spare_lens;
     ~dg_graph();
 };
 

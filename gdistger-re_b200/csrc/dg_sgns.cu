@@ -1735,10 +1735,10 @@ extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t 
     for (uint64_t i = 0; i < total; i++)
         DG_CHECK(vertices[i] < s->v_num, DG_ERR_ARG, "vertex %u >= v_num %u", vertices[i], s->v_num);
     dg::DeviceGuard guard(s->device);
-    dg::DevArray<uint64_t> d_off;
-    dg::DevArray<uint32_t> d_verts;
-    DG_CUDA(d_off.alloc((size_t)n_walks + 1));
-    DG_CUDA(d_verts.alloc(total ? total : 1));
+    dg::DevArray<uint64_t> &d_off = s->host_off;
+    dg::DevArray<uint32_t> &d_verts = s->host_verts;
+    if (d_off.n < (size_t)n_walks + 1) DG_CUDA(d_off.alloc((size_t)n_walks + 1 + n_walks / 8));
+    if (d_verts.n < (total ? total : 1)) DG_CUDA(d_verts.alloc((total ? total : 1) + total / 8));
     DG_CUDA(cudaMemcpyAsync(d_off.p, offsets, ((size_t)n_walks + 1) * 8, cudaMemcpyHostToDevice, s->stream));
     if (total) DG_CUDA(cudaMemcpyAsync(d_verts.p, vertices, total * 4, cudaMemcpyHostToDevice, s->stream));
     dgs::WalkSet ws{};

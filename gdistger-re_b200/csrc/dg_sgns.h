@@ -142,5 +142,7 @@ struct dg_sgns {
     uint64_t adj_exec_k = 0;
     dg::DevArray<uint32_t> queue;
     dg::DevArray<unsigned long long> stats;
+    dg::DevArray<uint64_t> host_off;     // dg_sgns_train_host: device copies of the caller's walks,
+    dg::DevArray<uint32_t> host_verts;   // kept (and grown) between calls
     ~dg_sgns();
 };

@@ -233,8 +233,8 @@ __global__ void compact_walks(const uint32_t *__restrict__ verts, const uint32_t
 
 int relative_entropy(dg_graph *g, uint64_t words_sum, double *h) {
     const int blocks = dg::sm_count(g->device) * 4;
-    dg::DevArray<double> partial;
-    DG_CUDA(partial.alloc(blocks));
+    dg::DevArray<double> &partial = g->entropy_partial;
+    if (partial.n < (size_t)blocks) DG_CUDA(partial.alloc(blocks));
     entropy_partials<<<blocks, kEntropyThreads, 0, g->stream>>>(g->out_deg.p, g->freq.p, g->v_num, (double)g->m,
                                                                   (double)words_sum, partial.p); dg::note_launch();
     DG_CUDA(cudaGetLastError());
@@ -289,18 +289,23 @@ int run_round(dg_graph *g, const dg_walk_params *p, uint32_t round, uint32_t n_w
     ps->round = round;
     ps->n_walks = n_walkers;
     ps->stride = stride;
-    DG_CUDA(ps->verts.alloc((size_t)n_walkers * stride));
-    DG_CUDA(ps->lens.alloc(n_walkers));
+    if (g->spare_verts.n >= (size_t)n_walkers * stride && g->spare_lens.n >= n_walkers) {
+        ps->verts.swap(g->spare_verts);   // the arena of a freed round (its walks are not read again)
+        ps->lens.swap(g->spare_lens);
+    } else {
+        DG_CUDA(ps->verts.alloc((size_t)n_walkers * stride));
+        DG_CUDA(ps->lens.alloc(n_walkers));
+    }
 
-    dg::DevArray<unsigned long long> stats;
-    dg::DevArray<uint32_t> ctl;  // [0] queue head, [1] longest walk
-    DG_CUDA(stats.alloc(4));
-    DG_CUDA(ctl.alloc(2));
+    dg::DevArray<unsigned long long> &stats = g->round_stats;
+    dg::DevArray<uint32_t> &ctl = g->round_ctl;  // [0] queue head, [1] longest walk
+    if (!stats.p) DG_CUDA(stats.alloc(4));
+    if (!ctl.p) DG_CUDA(ctl.alloc(2));
     DG_CUDA(cudaMemsetAsync(stats.p, 0, 4 * sizeof(unsigned long long), g->stream));
     DG_CUDA(cudaMemsetAsync(ctl.p, 0, 2 * sizeof(uint32_t), g->stream));
     // Keep the pre-round visit counts so a failed (overflowing) round can be undone.
-    dg::DevArray<uint32_t> freq_backup;
-    DG_CUDA(freq_backup.alloc(g->v_num));
+    dg::DevArray<uint32_t> &freq_backup = g->freq_backup;
+    if (freq_backup.n < g->v_num) DG_CUDA(freq_backup.alloc(g->v_num));
     DG_CUDA(cudaMemcpyAsync(freq_backup.p, g->freq.p, (size_t)g->v_num * 4, cudaMemcpyDeviceToDevice, g->stream));
 
     WalkArgs a;
@@ -443,6 +448,12 @@ extern "C" void dg_paths_free(dg_paths *ps) {
     if (!ps) return;
     dg::DeviceGuard guard(ps->device);
     cudaStreamSynchronize(ps->g->stream);
+    // The graph keeps the largest freed arena for its next round.
+    dg_graph *g = ps->g;
+    if (ps->verts.n > g->spare_verts.n) {
+        g->spare_verts.swap(ps->verts);
+        g->spare_lens.swap(ps->lens);
+    }
     delete ps;
 }
 

@@ -121,6 +121,8 @@ DG_API int dg_paths_copy(const dg_paths *paths, uint64_t *offsets, uint32_t *ver
  * The text is formatted on the device. */
 DG_API int dg_paths_write_text(const dg_paths *paths, const char *file_path);
 
+/* Frees the walks; call it before dg_graph_free of their graph.  The graph keeps
+ * the largest freed walk arena and reuses it for its next round. */
 DG_API void dg_paths_free(dg_paths *paths);
 
 /* Cumulative visit frequency per vertex over all rounds run on g. */

@@ -123,7 +123,7 @@ Options parse(int argc, char **argv) {
     if (o.graph.empty() || o.v_num == 0 || o.walker_num == 0)
         die("usage: huge_walk -g edges.bin -v V -w W [--min_L L] [--min_R R] [--make-undirected] [-o prefix] "
             "[-size d -window k -negative n -batch-size b -sample s -alpha a -iter i -min-count c "
-            "-emb_output file] [-mode plain|minibatch]");
+            "-emb_output file] [-mode plain|plain_bf16|minibatch]");
     if (o.mode != "plain" && o.mode != "minibatch" && o.mode != "plain_bf16")
         die("-mode must be plain, plain_bf16 or minibatch");
     if (o.rounds < 1 || o.rounds > 30) die("-rounds must be 1..30 (walk.hpp:740 stops after round 30)");

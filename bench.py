@@ -48,6 +48,7 @@ WORKLOAD = {"graph": "youtube-shaped chung-lu", "vertices": 1_138_499, "undirect
 # Algorithmic bytes per unit (roofline section).
 BYTES_PER_PAIR_PLAIN = lambda d, n: 2 * (2 + n) * d * 4          # noqa: E731  context + 1+n targets, read+write
 BYTES_PER_DRAW, BYTES_PER_FOOTPRINT = 28, 4
+BYTES_PER_ROW_MB = lambda d: 2 * d * 2                            # noqa: E731  BF16 row, read + write
 # Adjoint pass, per pair: rows read (input, positive output, negative/batch shared rows) at e bytes, the 8-byte
 # fixed-point accumulators read and written by the gradient kernel, then read and cleared by the step kernel,
 # which also reads and writes the row element.
@@ -271,7 +272,7 @@ def run_ours(args, rank, world, local, pg):
     torch.cuda.synchronize()
     l0 = L.dg_launch_count()
     tot_ms = walk_ms = train_ms = 0.0
-    fp = steps_ = draws = words = pairs = 0
+    fp = steps_ = draws = words = pairs = rows = 0
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
@@ -284,6 +285,7 @@ def run_ours(args, rank, world, local, pg):
         draws += info.walk.draws
         words += info.train.words
         pairs += info.train.pairs
+        rows += info.train.rows
     torch.cuda.synchronize()
     barrier(pg)
     launches = L.dg_launch_count() - l0
@@ -328,7 +330,9 @@ def run_ours(args, rank, world, local, pg):
     traffic = load_traffic()
     if train_ms >= walk_ms:
         kern = "sgns_plain" if mode == "plain" else "sgns_minibatch"
-        alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else None
+        # minibatch form: every step reads and writes its I input and O output rows
+        # at 2 bytes (the FP32 master rows counted at 2 bytes too)
+        alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else rows * BYTES_PER_ROW_MB(128)
         if mode == "plain_bf16":
             # rows at 2 bytes (the 65,536 FP32 master rows are counted at 2 bytes too)
             kern, alg = "sgns_plain_bf16", pairs * BYTES_PER_PAIR_PLAIN(128, 5) / 2
@@ -338,6 +342,9 @@ def run_ours(args, rank, world, local, pg):
         kms = train_ms
         per = traffic.get(kern, {}).get("dram_bytes_per_pair")
         tr = per * pairs / args.steps if per else None
+        per_word = traffic.get(kern, {}).get("dram_bytes_per_word")
+        if per_word:
+            tr = per_word * words / args.steps
     else:
         kern = "walk"
         alg = draws * BYTES_PER_DRAW + fp * BYTES_PER_FOOTPRINT

@@ -1585,6 +1585,7 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
         info->trained = st[1];
         info->pairs = st[2];
         info->train_ms = t.ms();
+        info->rows = st[3];
     }
     return DG_OK;
 }

@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D), mb_min_blocks(D)) sgns_mb_ke
     // Worker state, identical in every thread.
     int len[2] = {0, 0}, pos[2] = {0, 0};
     int nbn = 1;
-    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0, n_rows = 0;
     uint32_t next_walk = w_begin;
     uint32_t step = 0, pool_no = 0, neg_count = 0;
     int train_sen_num = 0;
@@ -449,6 +449,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D), mb_min_blocks(D)) sgns_mb_ke
         __syncthreads();
         const int O = shr[5], I = shr[6], first = shr[7];
         n_pairs += I;
+        n_rows += I + O;
 
         // ---- output rows into registers (centres from the tables, negatives from the pool) ----
         Cols<V> x[OUT];
@@ -608,6 +609,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D), mb_min_blocks(D)) sgns_mb_ke
         atomicAdd(&a.stats[0], n_words);
         atomicAdd(&a.stats[1], n_trained);
         atomicAdd(&a.stats[2], n_pairs);
+        atomicAdd(&a.stats[3], n_rows);
     }
 }
 
@@ -855,6 +857,7 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
         info->trained = st[1];
         info->pairs = st[2];
         info->train_ms = 0.0;
+        info->rows = st[3];
     }
     return DG_OK;
 }

@@ -49,7 +49,7 @@ class SgnsParams(C.Structure):
 
 class TrainInfo(C.Structure):
     _fields_ = [("words", C.c_uint64), ("trained", C.c_uint64), ("pairs", C.c_uint64),
-                ("train_ms", C.c_double)]
+                ("train_ms", C.c_double), ("rows", C.c_uint64)]
 
 
 class PipelineInfo(C.Structure):

@@ -176,6 +176,8 @@ typedef struct {
     uint64_t trained;    /* tokens kept after subsampling */
     uint64_t pairs;      /* (centre, context) pairs */
     double train_ms;     /* SGNS kernel time */
+    uint64_t rows;       /* minibatch form: input + output rows of every minibatch step, summed
+                            (dsgl.hpp:1089-1160); 0 for the other forms */
 } dg_train_info;
 
 /* One pass (x iter) over a round's walks with learning rate alpha (alpha <= 0:

@@ -1411,6 +1411,17 @@ __global__ void rows_to_f32(const __nv_bfloat16 *rows, const float *master, uint
         out[k] = k < n_master ? master[k] : __bfloat162float(rows[k]);
 }
 
+// Largest vertex id of a host-supplied walk set, checked on the device after the
+// copy instead of element by element on the host.
+__global__ void max_vertex_kernel(const uint32_t *v, uint64_t n, unsigned int *out) {
+    uint32_t m = 0;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x)
+        m = max(m, __ldg(v + k));
+#pragma unroll
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 __global__ void rows_from_f32(const float *in, uint64_t n, uint64_t n_master, __nv_bfloat16 *rows, float *master) {
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
         rows[k] = __float2bfloat16_rn(in[k]);
@@ -1733,15 +1744,26 @@ extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t 
                                   float alpha, dg_train_info *info) {
     DG_CHECK(s && offsets && (vertices || offsets[n_walks] == 0), DG_ERR_ARG, "dg_sgns_train_host: NULL argument");
     const uint64_t total = offsets[n_walks];
-    for (uint64_t i = 0; i < total; i++)
-        DG_CHECK(vertices[i] < s->v_num, DG_ERR_ARG, "vertex %u >= v_num %u", vertices[i], s->v_num);
+    for (uint32_t i = 0; i < n_walks; i++)
+        DG_CHECK(offsets[i + 1] >= offsets[i], DG_ERR_ARG, "walk offsets decrease at walk %u", i);
     dg::DeviceGuard guard(s->device);
     dg::DevArray<uint64_t> &d_off = s->host_off;
     dg::DevArray<uint32_t> &d_verts = s->host_verts;
     if (d_off.n < (size_t)n_walks + 1) DG_CUDA(d_off.alloc((size_t)n_walks + 1 + n_walks / 8));
     if (d_verts.n < (total ? total : 1)) DG_CUDA(d_verts.alloc((total ? total : 1) + total / 8));
     DG_CUDA(cudaMemcpyAsync(d_off.p, offsets, ((size_t)n_walks + 1) * 8, cudaMemcpyHostToDevice, s->stream));
-    if (total) DG_CUDA(cudaMemcpyAsync(d_verts.p, vertices, total * 4, cudaMemcpyHostToDevice, s->stream));
+    if (total) {
+        DG_CUDA(cudaMemcpyAsync(d_verts.p, vertices, total * 4, cudaMemcpyHostToDevice, s->stream));
+        if (!s->vmax.p) DG_CUDA(s->vmax.alloc(1));
+        DG_CUDA(cudaMemsetAsync(s->vmax.p, 0, sizeof(unsigned int), s->stream));
+        dgs::max_vertex_kernel<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(d_verts.p, total, s->vmax.p);
+        dg::note_launch();
+        DG_CUDA(cudaGetLastError());
+        unsigned int vmax = 0;
+        DG_CUDA(cudaMemcpyAsync(&vmax, s->vmax.p, sizeof(vmax), cudaMemcpyDeviceToHost, s->stream));
+        DG_CUDA(cudaStreamSynchronize(s->stream));
+        DG_CHECK(vmax < s->v_num, DG_ERR_ARG, "vertex %u >= v_num %u", vmax, s->v_num);
+    }
     dgs::WalkSet ws{};
     ws.verts = d_verts.p;
     ws.offsets = d_off.p;

@@ -144,5 +144,6 @@ struct dg_sgns {
     dg::DevArray<unsigned long long> stats;
     dg::DevArray<uint64_t> host_off;     // dg_sgns_train_host: device copies of the caller's walks,
     dg::DevArray<uint32_t> host_verts;   // kept (and grown) between calls
+    dg::DevArray<unsigned int> vmax;     // dg_sgns_train_host: largest vertex id of the call
     ~dg_sgns();
 };

@@ -132,6 +132,8 @@ struct dg_graph {
     dg::DevArray<uint32_t> round_ctl, freq_backup;
     dg::DevArray<double> entropy_partial;
     dg::DevArray<uint32_t> spare_verts, spare_lens;
+    dg::DevArray<uint64_t> copy_at;   // dg_paths_copy: walk offsets and compacted walks,
+    dg::DevArray<uint32_t> copy_flat; // kept (and grown) between calls
     ~dg_graph();
 };
 

@@ -394,21 +394,22 @@ extern "C" int dg_paths_get_info(const dg_paths *paths, dg_round_info *info) {
 extern "C" int dg_paths_copy(const dg_paths *ps, uint64_t *offsets, uint32_t *vertices) {
     DG_CHECK(ps, DG_ERR_ARG, "dg_paths_copy: NULL paths");
     dg::DeviceGuard guard(ps->device);
-    cudaStream_t s = ps->g->stream;
-    dg::DevArray<uint64_t> at;
-    DG_CUDA(at.alloc((size_t)ps->n_walks + 1));
+    dg_graph *g = ps->g;
+    cudaStream_t s = g->stream;
+    dg::DevArray<uint64_t> &at = g->copy_at;
+    if (at.n < (size_t)ps->n_walks + 1) DG_CUDA(at.alloc((size_t)ps->n_walks + 1));
     int rc = dg::exclusive_scan_u32_to_u64(ps->lens.p, at.p, ps->n_walks, s);
     if (rc) return rc;
-    if (offsets) DG_CUDA(cudaMemcpy(offsets, at.p, ((size_t)ps->n_walks + 1) * 8, cudaMemcpyDeviceToHost));
+    if (offsets) DG_CUDA(cudaMemcpyAsync(offsets, at.p, ((size_t)ps->n_walks + 1) * 8, cudaMemcpyDeviceToHost, s));
     if (vertices && ps->info.footprints) {
-        dg::DevArray<uint32_t> flat;
-        DG_CUDA(flat.alloc(ps->info.footprints));
+        dg::DevArray<uint32_t> &flat = g->copy_flat;
+        if (flat.n < ps->info.footprints) DG_CUDA(flat.alloc(ps->info.footprints + ps->info.footprints / 8));
         compact_walks<<<dg::sm_count(ps->device) * 8, 256, 0, s>>>(ps->verts.p, ps->lens.p, ps->n_walks, ps->stride,
                                                                      at.p, flat.p); dg::note_launch();
         DG_CUDA(cudaGetLastError());
-        DG_CUDA(cudaStreamSynchronize(s));
-        DG_CUDA(cudaMemcpy(vertices, flat.p, ps->info.footprints * 4, cudaMemcpyDeviceToHost));
+        DG_CUDA(cudaMemcpyAsync(vertices, flat.p, ps->info.footprints * 4, cudaMemcpyDeviceToHost, s));
     }
+    DG_CUDA(cudaStreamSynchronize(s));
     return DG_OK;
 }
 

@@ -114,7 +114,8 @@ DG_API int dg_walk_run_round(dg_graph *g, const dg_walk_params *p, uint32_t roun
 DG_API int dg_paths_get_info(const dg_paths *paths, dg_round_info *info);
 
 /* Copies walks in walker order: offsets[n_walks+1] (footprint offsets) and
- * vertices[footprints] (either may be NULL). */
+ * vertices[footprints] (either may be NULL).  The walks are compacted on the
+ * device into buffers the graph keeps for later calls. */
 DG_API int dg_paths_copy(const dg_paths *paths, uint64_t *offsets, uint32_t *vertices);
 
 /* Writes the walk file: per walk " %u" per vertex then "\n" (path.hpp:92,108).

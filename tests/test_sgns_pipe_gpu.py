@@ -89,3 +89,53 @@ def test_long_walks_fall_back(distger_lib, round1):
     assert np.isfinite(b.embedding()[0]).all()
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("size,negative,window", [(64, 3, 5), (128, 8, 15), (128, 5, 1)])
+def test_staged_other_instances(distger_lib, round1, size, negative, window):
+    """The staged kernel's other instances (any negative count <= 8, 64-float
+    rows, the widest window it takes, window 1) give the sequential pair counts
+    and a two-warp result as close to the sequential one as the unstaged kernel's."""
+    from distger.sgns import SGNS
+    p, counts = round1
+
+    def run(shape=None, **kw):
+        s = SGNS(10_000, counts, size=size, window=window, negative=negative, sample=1e-3, alpha=0.025,
+                 min_count=0, seed=3, table_size=1_000_000, **kw)
+        if shape is not None:
+            s.set_shape(shape)
+        info = s.train_paths(p)
+        out = (info, s.embedding()[0], s.output_rows())
+        s.close()
+        return out
+
+    seq = run(deterministic=True)
+    plain = run(shape=UNSTAGED, workers=2)
+    pipe = run(shape=STAGED2, workers=2)
+    for info in (plain[0], pipe[0]):
+        assert (info.words, info.trained, info.pairs) == (seq[0].words, seq[0].trained, seq[0].pairs)
+    d_plain = max(_rel(plain[1], seq[1]), _rel(plain[2], seq[2]))
+    d_pipe = max(_rel(pipe[1], seq[1]), _rel(pipe[2], seq[2]))
+    print(f"size {size} negative {negative} window {window}: staged {d_pipe:.3e}, unstaged {d_plain:.3e}")
+    assert np.isfinite(pipe[1]).all() and np.isfinite(pipe[2]).all()
+    assert d_pipe <= 3 * d_plain + 1e-4
+
+
+def test_staged_short_and_empty_walks(distger_lib, round1):
+    """Walks of 0, 1 and 2 tokens (no pairs, one pair each way) in the staged
+    kernel: the same counts as the sequential kernel."""
+    from distger.sgns import SGNS
+    _, counts = round1
+    rng = np.random.default_rng(3)
+    lens = rng.choice([0, 1, 2, 3, 25], size=3000)
+    offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.uint64)
+    verts = rng.integers(0, 10_000, size=int(offs[-1])).astype(np.uint32)
+    kw = dict(size=128, window=10, negative=5, sample=0, alpha=0.025, min_count=0, seed=3, table_size=1_000_000)
+    a = SGNS(10_000, counts, deterministic=True, **kw)
+    b = SGNS(10_000, counts, workers=2, **kw)
+    b.set_shape(STAGED2)
+    ia, ib = a.train_host(offs, verts), b.train_host(offs, verts)
+    assert (ia.words, ia.trained, ia.pairs) == (ib.words, ib.trained, ib.pairs)
+    assert _rel(b.embedding()[0], a.embedding()[0]) < 0.05
+    a.close()
+    b.close()

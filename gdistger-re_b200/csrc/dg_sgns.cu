@@ -523,292 +523,6 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(
     }
 }
 
-// ------------------------------------------ plain rule, rows staged ahead
-
-// Hogwild form of the plain rule whose row loads overlap the previous pairs'
-// arithmetic: while pair m computes, the rows of pair m + S - 1 (its context row
-// and its negatives' rows) are copied into this warp's shared memory with
-// cp.async, so a pair waits on a copy issued S - 1 pairs earlier instead of a
-// DRAM round trip.  Each lane copies, and later reads, only its own columns.
-// A copy made before this warp's last updates of the same row would miss them;
-// the kernel restores them where they matter:
-//  * context rows: a context word used by one of the previous S pairs is read
-//    from that pair's updated row (kept in shared memory), so a context row sees
-//    every update of this warp, as in sgns_plain_kernel;
-//  * the centre's output row is loaded when the centre starts (after every
-//    earlier update) and kept in registers, as in sgns_plain_kernel;
-//  * a negative's output row copied before one of the previous S pairs (or a
-//    finished centre) updated it misses that update: staleness of at most S
-//    pairs, of the kind other warps' concurrent updates cause in any Hogwild run.
-// Draws, pairs, sums, gradients and the update order of each pair are
-// sgns_plain_kernel's.  The launcher uses it only without `deterministic`, for
-// sentences of at most kPipeSentence tokens, window <= kPipeMaxWindow and
-// negative <= kFastNeg.
-constexpr uint32_t kPipeSentence = 64;
-constexpr int kPipeMaxWindow = 15;
-
-template <int VEC>
-__device__ __forceinline__ void copy_row_async(float *dst, const float *src) {
-    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst);
-    const size_t ga = __cvta_generic_to_global(src);
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4)
-            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa + 4 * i), "l"(ga + 4 * i) : "memory");
-    } else if constexpr (VEC == 2) {
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(ga) : "memory");
-    } else {
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(ga) : "memory");
-    }
-}
-
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
-// This lane's columns of a row held in shared memory.
-template <int VEC>
-__device__ __forceinline__ void lds_row(const float *p, RowVec<VEC> &r) {
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4) {
-            const float4 t = *reinterpret_cast<const float4 *>(p + i);
-            r.v[i] = t.x; r.v[i + 1] = t.y; r.v[i + 2] = t.z; r.v[i + 3] = t.w;
-        }
-    } else {
-#pragma unroll
-        for (int i = 0; i < VEC; i++) r.v[i] = p[i];
-    }
-}
-
-template <int VEC>
-__device__ __forceinline__ void sts_row(float *p, const RowVec<VEC> &r) {
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4)
-            *reinterpret_cast<float4 *>(p + i) = make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]);
-    } else {
-#pragma unroll
-        for (int i = 0; i < VEC; i++) p[i] = r.v[i];
-    }
-}
-
-template <int VEC, int NS, int S>
-struct alignas(16) PipeWarp {
-    float stage[S][1 + NS][32 * VEC];             // rows of S pairs: context, negatives 0..NS-1
-    float hist[S][32 * VEC];                      // updated context rows of the last S pairs
-    int32_t sen[kPipeSentence];
-    int32_t tb[S][(2 * kPipeMaxWindow + 1) * NS];  // negatives of S centres, ring by centre
-    uint16_t lohi[kPipeSentence];                 // slot range of each centre: lo | hi << 8
-};
-
-template <int VEC, int THREADS, int NEG, int S, int FIT>
-__global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_kernel(SgnsArgs a, WalkSet ws) {
-    constexpr int NS = NEG > 0 ? NEG : kFastNeg;
-    constexpr int D = 32 * VEC;
-    constexpr int M = pow2_at_least(NS + 1);
-    constexpr int GROUP = 32 / M;
-    __shared__ PipeWarp<VEC, NS, S> sm_all[THREADS / 32];
-    PipeWarp<VEC, NS, S> &sm = sm_all[threadIdx.x >> 5];
-    const uint32_t lane = threadIdx.x & 31;
-    const uint32_t w = (uint32_t)a.window;
-    const float alpha = a.alpha;
-    const int neg = NEG > 0 ? NEG : (a.vocab_size > 1 ? a.negative : 0);
-    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
-    int32_t hw[S];   // context words of this warp's last S pairs, newest first
-#pragma unroll
-    for (int k = 0; k < S; k++) hw[k] = -1;
-    uint32_t mm = 0;  // pairs trained by this warp (ring position of hist)
-    for (;;) {
-        uint32_t walk = 0;
-        if (lane == 0) walk = atomicAdd(a.queue, 1u);
-        walk = __shfl_sync(0xffffffffu, walk, 0);
-        if (walk >= ws.n_walks) break;
-        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
-        uint32_t words;
-        const uint32_t n = warp_sentence<kPipeSentence>(ws, walk, a, sm.sen, words);
-        n_words += words;
-        n_trained += n;
-        if (n < 2) continue;   // a one-token sentence has no pairs
-        for (uint32_t q = lane; q < n; q += 32) {
-            const uint32_t b = philox(q, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
-            uint32_t lo, hi;
-            slot_range(q, n, w, b, lo, hi);
-            sm.lohi[q] = (uint16_t)(lo | (hi << 8));
-        }
-        __syncwarp();
-        // With n >= 2 every centre has a pair, and slot w lies inside its range.
-        auto first_slot = [&](uint32_t q) {
-            const uint32_t s0 = sm.lohi[q] & 0xFFu;
-            return s0 == w ? s0 + 1 : s0;
-        };
-        auto advance = [&](uint32_t &q, uint32_t &s) {   // next pair; true when centre q ended
-            s++;
-            if (s == w) s++;
-            if (s < (uint32_t)(sm.lohi[q] >> 8)) return false;
-            q++;
-            if (q < n) s = first_slot(q);
-            return true;
-        };
-        auto enter = [&](uint32_t q) {   // the copies reach centre q: draw its negatives
-            const uint32_t lo = sm.lohi[q] & 0xFFu, hi = sm.lohi[q] >> 8;
-            draw_negatives(a, q, wid, lo, hi, neg, sm.tb[q % S], NS);
-            if (lane == 0) prefetch_l2(a.syn1 + (size_t)sm.sen[q] * D, (uint32_t)D * 4);
-        };
-        auto issue = [&](uint32_t q, uint32_t s, uint32_t st) {
-            const int32_t ctx = sm.sen[q - w + s];
-            copy_row_async<VEC>(&sm.stage[st][0][lane * VEC], a.syn0 + (size_t)ctx * D + lane * VEC);
-            const int32_t *tq = sm.tb[q % S] + (s - (sm.lohi[q] & 0xFFu)) * NS;
-#pragma unroll
-            for (int j = 0; j < NS; j++)
-                if (j < neg)
-                    copy_row_async<VEC>(&sm.stage[st][1 + j][lane * VEC], a.syn1 + (size_t)tq[j] * D + lane * VEC);
-        };
-        uint32_t pp = 0, sp = first_slot(0);   // next pair to copy
-        enter(0);
-#pragma unroll
-        for (int i = 0; i < S - 1; i++) {
-            if (pp < n) {
-                issue(pp, sp, (uint32_t)i);
-                if (advance(pp, sp) && pp < n) enter(pp);
-            }
-            cp_async_commit();
-        }
-        uint32_t p = 0, s = first_slot(0);     // pair to train
-        float *pos_row = a.syn1 + (size_t)sm.sen[0] * D + lane * VEC;
-        RowVec<VEC> pos, pos0;
-        load_row<VEC>(pos_row, pos);
-        pos0 = pos;
-        for (uint32_t m = 0; p < n; m++) {
-            if (pp < n) {
-                issue(pp, sp, (m + S - 1) % S);
-                if (advance(pp, sp) && pp < n) enter(pp);
-            }
-            cp_async_commit();
-            cp_async_wait<S - 1>();   // this lane's copies of pair m have landed
-            const uint32_t st = m % S;
-            const int32_t word = sm.sen[p];
-            const int32_t last = sm.sen[p - w + s];
-            RowVec<VEC> l1, e;
-            lds_row<VEC>(&sm.stage[st][0][lane * VEC], l1);
-#pragma unroll
-            for (int k = S - 1; k >= 0; k--)   // newest match last: it wins
-                if (hw[k] == last) lds_row<VEC>(&sm.hist[(mm + S - 1 - k) % S][lane * VEC], l1);
-            const int32_t *tq = sm.tb[p % S] + (s - (sm.lohi[p] & 0xFFu)) * NS;
-            int32_t t[NS];
-#pragma unroll
-            for (int j = 0; j < NS; j++) t[j] = j < neg ? tq[j] : -1;
-#pragma unroll
-            for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
-            n_pairs++;
-            bool repeat = false;
-#pragma unroll
-            for (int j = 0; j < NS; j++)
-#pragma unroll
-                for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
-            if (!repeat) {   // as in sgns_plain_kernel: all sums and gradients at once
-                float f[M], g[NS + 1];
-                {
-                    float s0 = 0.f;
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
-                    f[0] = s0;
-                }
-                uint32_t live = 0;
-#pragma unroll
-                for (int j = 0; j < NS; j++) {
-                    float sj = 0.f;
-                    if (j < neg) {
-                        RowVec<VEC> r;
-                        lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
-#pragma unroll
-                        for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], r.v[i], sj);
-                        if (t[j] != word) live |= 1u << j;
-                    }
-                    f[j + 1] = sj;
-                }
-#pragma unroll
-                for (int j = NS + 1; j < M; j++) f[j] = 0.f;
-                const float mine = warp_sums_split<M>(f, lane);
-                const uint32_t jm = lane / GROUP;
-                float gm = 0.f;
-                if (jm == 0) gm = sg_grad(mine, 1, a.exp_table, alpha);
-                else if (jm <= (uint32_t)NS && ((live >> (jm - 1)) & 1u)) gm = sg_grad(mine, 0, a.exp_table, alpha);
-#pragma unroll
-                for (int j = 0; j <= NS; j++) g[j] = __shfl_sync(0xffffffffu, gm, j * GROUP);
-#pragma unroll
-                for (int i = 0; i < VEC; i++) {
-                    e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
-                    pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
-                }
-#pragma unroll
-                for (int j = 0; j < NS; j++) {
-                    if (!((live >> j) & 1u)) continue;
-                    RowVec<VEC> r, upd;
-                    lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        e.v[i] = fmaf(g[j + 1], r.v[i], e.v[i]);
-                        upd.v[i] = __fmul_rn(g[j + 1], l1.v[i]);  // rounded product, never fused
-                    }
-                    add_row<VEC>(a.syn1 + (size_t)t[j] * D + lane * VEC, upd);
-                }
-            } else {   // a negative repeats: one target after the other
-                {
-                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < NS; j++) {
-                    if (j >= neg || t[j] == word) continue;
-                    RowVec<VEC> r, upd;
-                    lds_row<VEC>(&sm.stage[st][1 + j][lane * VEC], r);
-                    const float g = sg_grad(warp_dot<VEC>(l1, r), 0, a.exp_table, alpha);
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) {
-                        e.v[i] = fmaf(g, r.v[i], e.v[i]);
-                        upd.v[i] = __fmul_rn(g, l1.v[i]);
-                        r.v[i] += upd.v[i];
-                    }
-                    add_row<VEC>(a.syn1 + (size_t)t[j] * D + lane * VEC, upd);
-                    // A later negative of this pair on the same row sees this update.
-#pragma unroll
-                    for (int k = j + 1; k < NS; k++)
-                        if (t[k] == t[j]) sts_row<VEC>(&sm.stage[st][1 + k][lane * VEC], r);
-                }
-            }
-            add_row<VEC>(a.syn0 + (size_t)last * D + lane * VEC, e);
-#pragma unroll
-            for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
-            sts_row<VEC>(&sm.hist[mm % S][lane * VEC], l1);
-#pragma unroll
-            for (int k = S - 1; k > 0; k--) hw[k] = hw[k - 1];
-            hw[0] = last;
-            mm++;
-            if (advance(p, s)) {   // centre done: its output row's update, then the next centre's row
-#pragma unroll
-                for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
-                add_row<VEC>(pos_row, pos);
-                if (p < n) {
-                    pos_row = a.syn1 + (size_t)sm.sen[p] * D + lane * VEC;
-                    load_row<VEC>(pos_row, pos);
-                    pos0 = pos;
-                }
-            }
-        }
-    }
-    if (lane == 0) {
-        atomicAdd(&a.stats[0], n_words);
-        atomicAdd(&a.stats[1], n_trained);
-        atomicAdd(&a.stats[2], n_pairs);
-    }
-}
-
 // ---------------------------------------------------- plain rule, BF16 rows
 
 __device__ __forceinline__ uint32_t bf_mix(uint32_t h) {
@@ -907,6 +621,377 @@ struct BfRows {
         else store_bits(w, lane, v, salt);
     }
 };
+
+// ------------------------------------------ plain rule, rows staged ahead
+
+// Hogwild form of the plain rule whose row loads overlap the previous pairs'
+// arithmetic: while pair m computes, the rows of pair m + S - 1 (its context row
+// and its negatives' rows) are copied into this warp's shared memory with
+// cp.async, so a pair waits on a copy issued S - 1 pairs earlier instead of a
+// DRAM round trip.  Each lane copies, and later reads, only its own columns.
+// A copy made before this warp's last updates of the same row would miss them;
+// the kernel restores them where they matter:
+//  * context rows: a context word used by one of the previous S pairs is read
+//    from that pair's updated row (kept in shared memory), so a context row sees
+//    every update of this warp, as in sgns_plain_kernel;
+//  * the centre's output row is loaded when the centre starts (after every
+//    earlier update) and kept in registers, as in sgns_plain_kernel;
+//  * a negative's output row copied before one of the previous S pairs (or a
+//    finished centre) updated it misses that update: staleness of at most S
+//    pairs, of the kind other warps' concurrent updates cause in any Hogwild run.
+// Draws, pairs, sums, gradients and the update order of each pair are
+// sgns_plain_kernel's.  The launcher uses it only without `deterministic`, for
+// sentences of at most kPipeSentence tokens, window <= kPipeMaxWindow and
+// negative <= kFastNeg.
+constexpr uint32_t kPipeSentence = 64;
+constexpr int kPipeMaxWindow = 15;
+
+template <int VEC>
+__device__ __forceinline__ void copy_row_async(float *dst, const float *src) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst);
+    const size_t ga = __cvta_generic_to_global(src);
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa + 4 * i), "l"(ga + 4 * i) : "memory");
+    } else if constexpr (VEC == 2) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(ga) : "memory");
+    } else {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(ga) : "memory");
+    }
+}
+
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// This lane's columns of a row held in shared memory.
+template <int VEC>
+__device__ __forceinline__ void lds_row(const float *p, RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4) {
+            const float4 t = *reinterpret_cast<const float4 *>(p + i);
+            r.v[i] = t.x; r.v[i + 1] = t.y; r.v[i + 2] = t.z; r.v[i + 3] = t.w;
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) r.v[i] = p[i];
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void sts_row(float *p, const RowVec<VEC> &r) {
+    if constexpr (VEC % 4 == 0) {
+#pragma unroll
+        for (int i = 0; i < VEC; i += 4)
+            *reinterpret_cast<float4 *>(p + i) = make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]);
+    } else {
+#pragma unroll
+        for (int i = 0; i < VEC; i++) p[i] = r.v[i];
+    }
+}
+
+template <int VEC, int NS, int S>
+struct alignas(16) PipeWarp {
+    float stage[S][1 + NS][32 * VEC];             // rows of S pairs: context, negatives 0..NS-1
+    float hist[S][32 * VEC];                      // updated context rows of the last S pairs
+    int32_t sen[kPipeSentence];
+    int32_t tb[S][(2 * kPipeMaxWindow + 1) * NS];  // negatives of S centres, ring by centre
+    uint16_t lohi[kPipeSentence];                 // slot range of each centre: lo | hi << 8
+};
+
+// BF16 rows in a staging slot: this lane's VEC values at 2 bytes (the slot's
+// first 2 * VEC bytes).
+template <int VEC>
+__device__ __forceinline__ void copy_half_row_async(float *dst, const __nv_bfloat16 *src) {
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(dst);
+    const size_t ga = __cvta_generic_to_global(src);
+    if constexpr (VEC == 8) {
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(ga) : "memory");
+    } else if constexpr (VEC == 4) {
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(sa), "l"(ga) : "memory");
+    } else {
+        static_assert(VEC == 2, "BF16 staging supports 2, 4 or 8 values per lane");
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(sa), "l"(ga) : "memory");
+    }
+}
+
+template <int VEC>
+__device__ __forceinline__ void lds_half_row(const float *p, RowVec<VEC> &r) {
+    const uint32_t *q = reinterpret_cast<const uint32_t *>(p);
+#pragma unroll
+    for (int i = 0; i < VEC / 2; i++) {
+        const uint32_t t = q[i];
+        r.v[2 * i] = __uint_as_float(t << 16);
+        r.v[2 * i + 1] = __uint_as_float(t & 0xFFFF0000u);
+    }
+}
+
+// BF = false: FP32 rows (syn0, syn1), updates by vector atomics (DG_SGNS_PLAIN).
+// BF = true: the BF16 plain mode's rows and writes (BfRows: FP32 masters by
+// atomics, BF16 rows stored as the warp's updated copy with stochastic
+// rounding, the same noise keys as sgns_plain_bf16_kernel).  A BF16 row is
+// written back as (staged copy + update), so a concurrent update made since
+// the copy is lost; the launcher stages BF16 rows only where such collisions
+// are rare (dg_sgns::bf_staged).
+template <int VEC, int THREADS, int NEG, int S, int FIT, bool BF>
+__global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_kernel(SgnsArgs a, WalkSet ws) {
+    constexpr int NS = NEG > 0 ? NEG : kFastNeg;
+    constexpr int D = 32 * VEC;
+    constexpr int M = pow2_at_least(NS + 1);
+    constexpr int GROUP = 32 / M;
+    __shared__ PipeWarp<VEC, NS, S> sm_all[THREADS / 32];
+    PipeWarp<VEC, NS, S> &sm = sm_all[threadIdx.x >> 5];
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t w = (uint32_t)a.window;
+    const float alpha = a.alpha;
+    const int neg = NEG > 0 ? NEG : (a.vocab_size > 1 ? a.negative : 0);
+    const BfRows<VEC> in{a.in_bf, a.in_master, a.n_master, D};
+    const BfRows<VEC> out{a.out_bf, a.out_master, a.n_master, D};
+    const uint32_t key = a.seed_lo ^ bf_mix(a.pass * 0x9E3779B9u + 0x2F6B3A91u);
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    int32_t hw[S];   // context words of this warp's last S pairs, newest first
+#pragma unroll
+    for (int k = 0; k < S; k++) hw[k] = -1;
+    uint32_t mm = 0;  // pairs trained by this warp (ring position of hist)
+    // Copy of row `id` of the input (context) or output table into a staging slot.
+    auto copy_in = [&](float *dst, int32_t id, bool input) {
+        if constexpr (!BF) {
+            copy_row_async<VEC>(dst, (input ? a.syn0 : a.syn1) + (size_t)id * D + lane * VEC);
+        } else {
+            if ((uint32_t)id < a.n_master)
+                copy_row_async<VEC>(dst, (input ? a.in_master : a.out_master) + (size_t)id * D + lane * VEC);
+            else
+                copy_half_row_async<VEC>(dst, (input ? a.in_bf : a.out_bf) + (size_t)id * D + lane * VEC);
+        }
+    };
+    // A staged row of `id`; f32 = the slot holds FP32 values whatever the row's storage.
+    auto read_slot = [&](const float *src, int32_t id, bool f32, RowVec<VEC> &r) {
+        if (!BF || f32 || (uint32_t)id < a.n_master) lds_row<VEC>(src, r);
+        else lds_half_row<VEC>(src, r);
+    };
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence<kPipeSentence>(ws, walk, a, sm.sen, words);
+        n_words += words;
+        n_trained += n;
+        if (n < 2) continue;   // a one-token sentence has no pairs
+        for (uint32_t q = lane; q < n; q += 32) {
+            const uint32_t b = philox(q, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
+            uint32_t lo, hi;
+            slot_range(q, n, w, b, lo, hi);
+            sm.lohi[q] = (uint16_t)(lo | (hi << 8));
+        }
+        __syncwarp();
+        // With n >= 2 every centre has a pair, and slot w lies inside its range.
+        auto first_slot = [&](uint32_t q) {
+            const uint32_t s0 = sm.lohi[q] & 0xFFu;
+            return s0 == w ? s0 + 1 : s0;
+        };
+        auto advance = [&](uint32_t &q, uint32_t &s) {   // next pair; true when centre q ended
+            s++;
+            if (s == w) s++;
+            if (s < (uint32_t)(sm.lohi[q] >> 8)) return false;
+            q++;
+            if (q < n) s = first_slot(q);
+            return true;
+        };
+        auto enter = [&](uint32_t q) {   // the copies reach centre q: draw its negatives
+            const uint32_t lo = sm.lohi[q] & 0xFFu, hi = sm.lohi[q] >> 8;
+            draw_negatives(a, q, wid, lo, hi, neg, sm.tb[q % S], NS);
+            if (lane == 0) {
+                const int32_t cw = sm.sen[q];
+                if (!BF) prefetch_l2(a.syn1 + (size_t)cw * D, (uint32_t)D * 4);
+                else if ((uint32_t)cw < a.n_master) prefetch_l2(a.out_master + (size_t)cw * D, (uint32_t)D * 4);
+                else prefetch_l2(a.out_bf + (size_t)cw * D, (uint32_t)D * 2);
+            }
+        };
+        auto issue = [&](uint32_t q, uint32_t s, uint32_t st) {
+            copy_in(&sm.stage[st][0][lane * VEC], sm.sen[q - w + s], true);
+            const int32_t *tq = sm.tb[q % S] + (s - (sm.lohi[q] & 0xFFu)) * NS;
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+                if (j < neg) copy_in(&sm.stage[st][1 + j][lane * VEC], tq[j], false);
+        };
+        // The centre's output row, kept in registers while the centre trains.
+        auto load_pos = [&](int32_t cw, RowVec<VEC> &r) {
+            if constexpr (BF) out.load(cw, lane, r);
+            else load_row<VEC>(a.syn1 + (size_t)cw * D + lane * VEC, r);
+        };
+        auto centre_noise = [&](uint32_t q) {   // sgns_plain_bf16_kernel's per-centre noise base
+            return bf_mix(key ^ bf_mix(wid * 0x01000193u + q * 0x2545F491u) ^ lane * 0x85EBCA6Bu);
+        };
+        uint32_t pp = 0, sp = first_slot(0);   // next pair to copy
+        enter(0);
+#pragma unroll
+        for (int i = 0; i < S - 1; i++) {
+            if (pp < n) {
+                issue(pp, sp, (uint32_t)i);
+                if (advance(pp, sp) && pp < n) enter(pp);
+            }
+            cp_async_commit();
+        }
+        uint32_t p = 0, s = first_slot(0);     // pair to train
+        int32_t word = sm.sen[0];
+        uint32_t base = BF ? centre_noise(0) : 0u;
+        RowVec<VEC> pos, pos0;
+        load_pos(word, pos);
+        pos0 = pos;
+        for (uint32_t m = 0; p < n; m++) {
+            if (pp < n) {
+                issue(pp, sp, (m + S - 1) % S);
+                if (advance(pp, sp) && pp < n) enter(pp);
+            }
+            cp_async_commit();
+            cp_async_wait<S - 1>();   // this lane's copies of pair m have landed
+            const uint32_t st = m % S;
+            const int32_t last = sm.sen[p - w + s];
+            RowVec<VEC> l1, e;
+            read_slot(&sm.stage[st][0][lane * VEC], last, false, l1);
+#pragma unroll
+            for (int k = S - 1; k >= 0; k--)   // newest match last: it wins
+                if (hw[k] == last) lds_row<VEC>(&sm.hist[(mm + S - 1 - k) % S][lane * VEC], l1);
+            const int32_t *tq = sm.tb[p % S] + (s - (sm.lohi[p] & 0xFFu)) * NS;
+            int32_t t[NS];
+#pragma unroll
+            for (int j = 0; j < NS; j++) t[j] = j < neg ? tq[j] : -1;
+#pragma unroll
+            for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
+            n_pairs++;
+            bool repeat = false;
+#pragma unroll
+            for (int j = 0; j < NS; j++)
+#pragma unroll
+                for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
+            // Writes negative j's row: an atomic delta (FP32 rows, masters) or the
+            // warp's updated copy (BF16 rows).
+            auto write_neg = [&](int j, const RowVec<VEC> &upd, const RowVec<VEC> &value) {
+                if constexpr (BF) out.update(t[j], lane, upd, value, base + (uint32_t)t[j] * 0x27D4EB2Fu + s * 16u + (uint32_t)j);
+                else add_row<VEC>(a.syn1 + (size_t)t[j] * D + lane * VEC, upd);
+            };
+            if (!repeat) {   // as in sgns_plain_kernel: all sums and gradients at once
+                float f[M], g[NS + 1];
+                {
+                    float s0 = 0.f;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
+                    f[0] = s0;
+                }
+                uint32_t live = 0;
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    float sj = 0.f;
+                    if (j < neg) {
+                        RowVec<VEC> r;
+                        read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], false, r);
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], r.v[i], sj);
+                        if (t[j] != word) live |= 1u << j;
+                    }
+                    f[j + 1] = sj;
+                }
+#pragma unroll
+                for (int j = NS + 1; j < M; j++) f[j] = 0.f;
+                const float mine = warp_sums_split<M>(f, lane);
+                const uint32_t jm = lane / GROUP;
+                float gm = 0.f;
+                if (jm == 0) gm = sg_grad(mine, 1, a.exp_table, alpha);
+                else if (jm <= (uint32_t)NS && ((live >> (jm - 1)) & 1u)) gm = sg_grad(mine, 0, a.exp_table, alpha);
+#pragma unroll
+                for (int j = 0; j <= NS; j++) g[j] = __shfl_sync(0xffffffffu, gm, j * GROUP);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) {
+                    e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
+                    pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                }
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    if (!((live >> j) & 1u)) continue;
+                    RowVec<VEC> r, upd;
+                    read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], false, r);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g[j + 1], r.v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g[j + 1], l1.v[i]);  // rounded product, never fused
+                        if (BF) r.v[i] += upd.v[i];
+                    }
+                    write_neg(j, upd, r);
+                }
+            } else {   // a negative repeats: one target after the other
+                {
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, pos.v[i], e.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                    }
+                }
+                uint32_t f32 = 0;   // bit k: slot k was rewritten with FP32 values
+#pragma unroll
+                for (int j = 0; j < NS; j++) {
+                    if (j >= neg || t[j] == word) continue;
+                    RowVec<VEC> r, upd;
+                    read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], (f32 >> j) & 1u, r);
+                    const float g = sg_grad(warp_dot<VEC>(l1, r), 0, a.exp_table, alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, r.v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, l1.v[i]);
+                        r.v[i] += upd.v[i];
+                    }
+                    write_neg(j, upd, r);
+                    // A later negative of this pair on the same row sees this update.
+#pragma unroll
+                    for (int k = j + 1; k < NS; k++)
+                        if (t[k] == t[j]) {
+                            sts_row<VEC>(&sm.stage[st][1 + k][lane * VEC], r);
+                            f32 |= 1u << k;
+                        }
+                }
+            }
+            if constexpr (BF) {
+                RowVec<VEC> v1;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) v1.v[i] = l1.v[i] + e.v[i];
+                in.update(last, lane, e, v1, base + (uint32_t)last * 0x165667B1u + s * 16u + 15u);
+            } else {
+                add_row<VEC>(a.syn0 + (size_t)last * D + lane * VEC, e);
+            }
+#pragma unroll
+            for (int i = 0; i < VEC; i++) l1.v[i] += e.v[i];
+            sts_row<VEC>(&sm.hist[mm % S][lane * VEC], l1);
+#pragma unroll
+            for (int k = S - 1; k > 0; k--) hw[k] = hw[k - 1];
+            hw[0] = last;
+            mm++;
+            if (advance(p, s)) {   // centre done: its output row's update, then the next centre's row
+                RowVec<VEC> delta;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) delta.v[i] = pos.v[i] - pos0.v[i];
+                if constexpr (BF) out.update(word, lane, delta, pos, base + (uint32_t)word * 0xD3A2646Cu + 0x5BD1E995u);
+                else add_row<VEC>(a.syn1 + (size_t)word * D + lane * VEC, delta);
+                if (p < n) {
+                    word = sm.sen[p];
+                    if (BF) base = centre_noise(p);
+                    load_pos(word, pos);
+                    pos0 = pos;
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
 
 // The plain kernel's schedule and update rule (word2vec.cu:305-399) on BF16
 // rows: the same pairs, draws and update order as sgns_plain_kernel, arithmetic
@@ -1279,6 +1364,29 @@ int adjoint_pairs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
     return DG_OK;
 }
 
+// Staged BF16 rows (sgns_plain_pipe_kernel<..., true>) are written back as the
+// warp's (copy + update), so an update another warp made to the row since the
+// copy is lost.  They are used only when the hottest BF16 row (vocabulary id
+// n_master; the vocabulary is sorted by count) is expected to be held by at
+// most kBfStagedHolders pairs in flight at once: 24 resident warps per SM, 2
+// pairs each, holding it as one of `negative` draws (unigram^0.75 share) or as
+// a context or centre token (twice its token share).  The YouTube-shaped
+// vocabulary gives 0.10; a 10,000-word table with 1,000 FP32 masters gives 8.
+constexpr double kBfStagedHolders = 0.5;
+
+bool bf_staging_safe(const std::vector<uint32_t> &cn, uint32_t n_master, int negative, int sms) {
+    if (n_master >= cn.size()) return true;   // every row an FP32 master (atomic updates)
+    double pow_sum = 0.0, tok_sum = 0.0;
+    for (uint32_t c : cn) {
+        pow_sum += std::pow((double)c, 0.75);
+        tok_sum += c;
+    }
+    if (!(pow_sum > 0) || !(tok_sum > 0)) return false;
+    const double c = cn[n_master];
+    const double holders = (double)sms * 24.0 * 2.0 * (negative * std::pow(c, 0.75) / pow_sum + 2.0 * c / tok_sum);
+    return holders <= kBfStagedHolders;
+}
+
 // An explicit worker count (warps) lowers the resident grid, never raises it.
 static int plain_blocks(const dg_sgns *s, int resident, int threads) {
     if (s->p.workers == 0) return resident;
@@ -1305,12 +1413,19 @@ static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) 
     const bool neg_fixed = a.negative == kPlainNeg && a.vocab_size > 1;
     if constexpr (BF) {
         kern = neg_fixed ? sgns_plain_bf16_kernel<V, T, kPlainNeg, FIT> : sgns_plain_bf16_kernel<V, T, 0, FIT>;
+        if constexpr (STG >= 2 && V == 4) {
+            if (s->bf_staged && pipe_applies(s, a, ws)) {
+                kern = neg_fixed ? sgns_plain_pipe_kernel<V, T, kPlainNeg, STG, FIT, true>
+                                 : sgns_plain_pipe_kernel<V, T, 0, STG, FIT, true>;
+                staged = true;
+            }
+        }
     } else {
         kern = neg_fixed ? sgns_plain_kernel<V, T, kPlainNeg, FIT> : sgns_plain_kernel<V, T, 0, FIT>;
         if constexpr (STG >= 2 && (V == 2 || V == 4)) {
             if (pipe_applies(s, a, ws)) {
-                kern = neg_fixed ? sgns_plain_pipe_kernel<V, T, kPlainNeg, STG, FIT>
-                                 : sgns_plain_pipe_kernel<V, T, 0, STG, FIT>;
+                kern = neg_fixed ? sgns_plain_pipe_kernel<V, T, kPlainNeg, STG, FIT, false>
+                                 : sgns_plain_pipe_kernel<V, T, 0, STG, FIT, false>;
                 staged = true;
             }
         }
@@ -1524,6 +1639,8 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
         DG_CUDA(cudaMemsetAsync(s->syn1.p, 0, n * 4, s->stream));
     } else {
         s->n_master = std::min<uint32_t>(s->vocab_size, p->master_rows ? p->master_rows : kMasterRows);
+        if (p->mode == DG_SGNS_PLAIN_BF16) s->bf_staged = bf_staging_safe(s->vocab_cn, s->n_master, p->negative,
+                                                                            dg::sm_count(device));
         const uint64_t nm = (uint64_t)s->n_master * p->size;
         DG_CUDA(s->in_bf.alloc(n));
         DG_CUDA(s->out_bf.alloc(n));
@@ -1805,6 +1922,7 @@ extern "C" int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info) {
     DG_CHECK(s && info, DG_ERR_ARG, "dg_sgns_get_info: NULL argument");
     info->vocab_size = s->vocab_size;
     info->master_rows = s->n_master;
+    info->bf_staged = s->bf_staged ? 1 : 0;
     info->workers = s->p.workers ? s->p.workers : s->p.deterministic == 2 ? s->adj_step_batches : s->mb_workers;
     info->train_words = s->train_words;
     info->table_size = s->p.table_size;

@@ -80,6 +80,7 @@ struct SgnsArgs {
 };
 
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+bool bf_staging_safe(const std::vector<uint32_t> &cn, uint32_t n_master, int negative, int sms);
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 
 // Concurrency bound of the minibatch form from the vocabulary (counts in
@@ -118,6 +119,7 @@ struct dg_sgns {
     uint32_t n_master = 0;
     uint32_t mb_workers = 0;           // minibatch form: staleness bound on concurrent workers
     int plain_shape = 0;               // plain form: launch shape (dg_sgns_autotune)
+    bool bf_staged = false;            // BF16 plain mode: rows may be staged (dgs::bf_staging_safe)
     uint64_t train_words = 0;
     uint32_t pass = 0;
     std::vector<uint32_t> vocab_ids, vocab_cn;

@@ -70,7 +70,7 @@ class MinibatchArgs(C.Structure):
 class SgnsInfo(C.Structure):
     _fields_ = [("vocab_size", C.c_uint32), ("master_rows", C.c_uint32), ("workers", C.c_uint32),
                 ("train_words", C.c_uint64),
-                ("table_size", C.c_uint64), ("device_bytes", C.c_uint64)]
+                ("table_size", C.c_uint64), ("device_bytes", C.c_uint64), ("bf_staged", C.c_int32)]
 
 
 class SgnsPairs(C.Structure):

@@ -44,6 +44,7 @@ class SGNS:
         self.vocab_size = info.vocab_size
         self.master_rows = info.master_rows
         self.workers = info.workers
+        self.bf_staged = bool(info.bf_staged)
         self.train_words = info.train_words
         self.table_size = info.table_size
 

@@ -209,6 +209,8 @@ typedef struct {
     uint64_t train_words;  /* sum of the vocabulary counts */
     uint64_t table_size;
     uint64_t device_bytes;
+    int32_t bf_staged;     /* BF16 plain mode: 1 if the default launch shape stages BF16 rows in shared
+                              memory (only when concurrent writers of one BF16 row are rare) */
 } dg_sgns_info;
 DG_API int dg_sgns_get_info(const dg_sgns *s, dg_sgns_info *info);
 DG_API int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float *output_rows);

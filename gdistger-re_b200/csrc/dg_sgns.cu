@@ -189,33 +189,6 @@ __device__ __forceinline__ float warp_dot(const RowVec<VEC> &a, const RowVec<VEC
     return s;
 }
 
-// Warp sums of M per-lane partials v[0..M) (M a power of two <= 32) for the cost
-// of about one: each halving stage sends half of the values still held to the
-// partner lane and keeps the other half, so after log2(M) stages lane l holds
-// one value, index l >> (5 - log2 M), summed over its lane group; plain
-// butterfly stages finish it.  Every addition is the one warp_dot's butterfly
-// makes for that value (own partial + partner's, then the same tree), so each
-// sum is bit-identical to warp_dot's.  Returns the held sum; v is clobbered.
-template <int M>
-__device__ __forceinline__ float warp_sums_split(float (&v)[M], uint32_t lane) {
-    static_assert(M >= 1 && M <= 32 && (M & (M - 1)) == 0, "M must be a power of two <= 32");
-#pragma unroll
-    for (int m = M, o = 16; m > 1; m >>= 1, o >>= 1) {
-        const bool up = (lane & (uint32_t)o) != 0;
-#pragma unroll
-        for (int k = 0; k < m / 2; k++) {
-            const float send = up ? v[k] : v[k + m / 2];
-            const float keep = up ? v[k + m / 2] : v[k];
-            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
-        }
-    }
-    float s = v[0];
-#pragma unroll
-    for (int o = 16 / M; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : 2 * pow2_at_least((x + 1) / 2); }
 
 // g = (label - sigmoid(f)) * alpha through expTable (word2vec.cu:383-388), with
 // the reference's integer-division index scale (EXP_TABLE_SIZE / MAX_EXP / 2 = 83).

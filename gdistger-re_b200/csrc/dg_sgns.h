@@ -79,6 +79,35 @@ struct SgnsArgs {
     int deterministic;
 };
 
+// Warp sums of M per-lane partials v[0..M) (M a power of two <= 32) for the cost
+// of about one: each halving stage sends half of the values still held to the
+// partner lane and keeps the other half, so after log2(M) stages lane l holds
+// one value, index l >> (5 - log2 M), summed over its lane group; plain
+// butterfly stages finish it.  Every addition is the one the plain butterfly
+// (s += shfl_xor(s, o), o = 16 .. 1) makes for that value (own partial +
+// partner's, then the same tree), so each sum is bit-identical to the plain
+// butterfly's.  Returns the held sum; v is clobbered.
+template <int M>
+__device__ __forceinline__ float warp_sums_split(float (&v)[M], uint32_t lane) {
+    static_assert(M >= 1 && M <= 32 && (M & (M - 1)) == 0, "M must be a power of two <= 32");
+#pragma unroll
+    for (int m = M, o = 16; m > 1; m >>= 1, o >>= 1) {
+        const bool up = (lane & (uint32_t)o) != 0;
+#pragma unroll
+        for (int k = 0; k < m / 2; k++) {
+            const float send = up ? v[k] : v[k + m / 2];
+            const float keep = up ? v[k + m / 2] : v[k];
+            v[k] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+        }
+    }
+    float s = v[0];
+#pragma unroll
+    for (int o = 16 / M; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    return s;
+}
+
+constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : 2 * pow2_at_least((x + 1) / 2); }
+
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 bool bf_staging_safe(const std::vector<uint32_t> &cn, uint32_t n_master, int negative, int sms);
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);

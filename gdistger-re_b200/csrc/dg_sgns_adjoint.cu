@@ -35,6 +35,7 @@ namespace dgs {
 namespace {
 
 constexpr int kAdjMaxNeg = 16;
+constexpr int kAdjFixedNeg = 5;                          // negative count with its own kernel instance
 constexpr float kFixScale = 1099511627776.0f;           // 2^40
 constexpr double kFixInv = 1.0 / 1099511627776.0;       // 2^-40
 constexpr float kFixMaxTerm = 1048576.0f;               // 2^20
@@ -94,12 +95,16 @@ __device__ __forceinline__ void fix_add(unsigned long long *p, float x, unsigned
 
 __device__ __forceinline__ float fix_value(unsigned long long q) { return (float)((double)(long long)q * kFixInv); }
 
-template <int V>
+// NEG > 0: the negative count fixed at compile time (a.negative == NEG); the
+// 1 + NEG dot products of a pair are then reduced together (warp_sums_split,
+// bit-identical to adj_dot) and each lane group evaluates one sigmoid.
+// NEG == 0: any count up to kAdjMaxNeg, one target after the other.
+template <int V, int NEG>
 __global__ void __launch_bounds__(kAdjThreads) sgns_adjoint_kernel(AdjArgs a) {
     constexpr int D = 32 * V;
     extern __shared__ __align__(16) float adj_smem[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, col = lane * V;
-    const int neg = a.negative;
+    const int neg = NEG > 0 ? NEG : a.negative;
     float *uk = adj_smem + (size_t)wib * 2 * neg * D;   // [neg][D] negative rows
     float *gk = uk + (size_t)neg * D;                    // [neg][D] their gradient sums
     uint64_t n_pairs = a.n_pairs, b_begin = a.b_begin, b_end = a.b_end;
@@ -142,6 +147,57 @@ __global__ void __launch_bounds__(kAdjThreads) sgns_adjoint_kernel(AdjArgs a) {
             }
             float v[V], dv[V];
             adj_load<V>(a.in_f32, a.in_bf, a.in_master, a.n_master, i, col, v);
+            if constexpr (NEG > 0) {
+                constexpr int M = pow2_at_least(NEG + 1);
+                constexpr int GROUP = 32 / M;
+                float f[M], u[NEG][V];
+                {
+                    float s0 = 0.f;
+#pragma unroll
+                    for (int c = 0; c < V; c++) s0 = fmaf(v[c], uo[c], s0);
+                    f[0] = s0;
+                }
+#pragma unroll
+                for (int k = 0; k < NEG; k++) {
+                    float sk = 0.f;
+#pragma unroll
+                    for (int c = 0; c < V; c++) {
+                        u[k][c] = uk[k * D + col + c];
+                        sk = fmaf(v[c], u[k][c], sk);
+                    }
+                    f[k + 1] = sk;
+                }
+#pragma unroll
+                for (int k = NEG + 1; k < M; k++) f[k] = 0.f;
+                const float mine = warp_sums_split<M>(f, (uint32_t)lane);
+                const int jm = lane / GROUP;
+                // sigmoid(s) - 1 for the positive target, sigmoid(s_k) for negative k
+                const float gm = jm == 0 ? -1.f / (1.f + expf(mine)) : jm <= NEG ? 1.f / (1.f + expf(-mine)) : 0.f;
+                float g[NEG + 1];
+#pragma unroll
+                for (int k = 0; k <= NEG; k++) g[k] = __shfl_sync(0xffffffffu, gm, k * GROUP);
+                if (a.batch_loss) {   // the loss in the sequential order (every lane holds every sum)
+                    loss += softplus(-(double)__shfl_sync(0xffffffffu, mine, 0));
+#pragma unroll
+                    for (int k = 0; k < NEG; k++) loss += softplus((double)__shfl_sync(0xffffffffu, mine, (k + 1) * GROUP));
+                }
+#pragma unroll
+                for (int c = 0; c < V; c++) {
+                    dv[c] = __fmul_rn(g[0], uo[c]);
+                    duo[c] = fmaf(g[0], v[c], duo[c]);
+                }
+#pragma unroll
+                for (int k = 0; k < NEG; k++) {
+#pragma unroll
+                    for (int c = 0; c < V; c++) {
+                        dv[c] = fmaf(g[k + 1], u[k][c], dv[c]);
+                        gk[k * D + col + c] = fmaf(g[k + 1], v[c], gk[k * D + col + c]);
+                    }
+                }
+#pragma unroll
+                for (int c = 0; c < V; c++) fix_add(a.acc_in + (size_t)i * D + col + c, dv[c], a.flag);
+                continue;
+            }
             const float s = adj_dot<V>(v, uo);
             const float g = -1.f / (1.f + expf(s));   // sigmoid(s) - 1
             if (a.batch_loss) loss += softplus(-(double)s);
@@ -275,9 +331,10 @@ int adjoint_config(dg_sgns *s, int negative, uint64_t n_batches, AdjLaunch &l) {
     while (warps > 1 && per_warp * warps > 96 * 1024) warps /= 2;
     l.smem = per_warp * warps;
     l.threads = warps * 32;
-    DG_CUDA(cudaFuncSetAttribute(sgns_adjoint_kernel<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
+    void (*kern)(AdjArgs) = negative == kAdjFixedNeg ? sgns_adjoint_kernel<V, kAdjFixedNeg> : sgns_adjoint_kernel<V, 0>;
+    DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)l.smem));
     int per_sm = 0;
-    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sgns_adjoint_kernel<V>, l.threads, l.smem));
+    DG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, l.threads, l.smem));
     const uint64_t need = (n_batches + warps - 1) / warps;
     l.blocks = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>(need, (uint64_t)dg::sm_count(s->device) * std::max(per_sm, 1)));
@@ -296,13 +353,19 @@ int adjoint_configure(dg_sgns *s, int negative, uint64_t n_batches, AdjLaunch &l
 }
 
 // Kernel launch only (no runtime calls besides the launch: safe inside a stream capture).
+template <int V>
+static void adjoint_enqueue_v(dg_sgns *s, const AdjLaunch &l, const AdjArgs &a) {
+    if (a.negative == kAdjFixedNeg) sgns_adjoint_kernel<V, kAdjFixedNeg><<<l.blocks, l.threads, l.smem, s->stream>>>(a);
+    else sgns_adjoint_kernel<V, 0><<<l.blocks, l.threads, l.smem, s->stream>>>(a);
+}
+
 void adjoint_enqueue(dg_sgns *s, const AdjLaunch &l, const AdjArgs &a) {
     switch (s->p.size) {
-    case 32: sgns_adjoint_kernel<1><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
-    case 64: sgns_adjoint_kernel<2><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
-    case 128: sgns_adjoint_kernel<4><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
-    case 256: sgns_adjoint_kernel<8><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
-    default: sgns_adjoint_kernel<16><<<l.blocks, l.threads, l.smem, s->stream>>>(a); break;
+    case 32: adjoint_enqueue_v<1>(s, l, a); break;
+    case 64: adjoint_enqueue_v<2>(s, l, a); break;
+    case 128: adjoint_enqueue_v<4>(s, l, a); break;
+    case 256: adjoint_enqueue_v<8>(s, l, a); break;
+    default: adjoint_enqueue_v<16>(s, l, a); break;
     }
 }
 

@@ -73,6 +73,52 @@ double entropy_term(double Sn, double fi) {
     return std::log2(a * b);
 }
 
+// First record (lowest index) that the reference would reject: a vertex id >=
+// v_num (graph.hpp:639 asserts) or data the transition's (int) conversion cannot
+// hold (walk.hpp:920).
+__global__ void check_records(const HostEdge *__restrict__ e, uint64_t n, uint32_t v_num, unsigned long long *bad) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const HostEdge r = e[i];
+        const bool ok = r.src < v_num && r.dst < v_num && isfinite(r.data) && r.data > -2147483648.0f &&
+                        r.data < 2147483648.0f;
+        if (!ok) atomicMin(bad, (unsigned long long)i);
+    }
+}
+
+// CSR entries in emission order: record i gives entry i (directed) or entries 2i
+// (src -> dst) and 2i + 1 (dst -> src) (graph.hpp:671-686); row = source, value
+// = data bits << 32 | neighbour.  Degrees are counted on the way.
+__global__ void emit_entries(const HostEdge *__restrict__ e, uint64_t n, int undirected, uint32_t *rows,
+                             unsigned long long *vals, uint32_t *out_deg, uint32_t *in_deg) {
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const HostEdge r = e[i];
+        const unsigned long long bits = (unsigned long long)__float_as_uint(r.data) << 32;
+        const uint64_t k = undirected ? 2 * i : i;
+        rows[k] = r.src;
+        vals[k] = bits | r.dst;
+        atomicAdd(&out_deg[r.src], 1u);
+        atomicAdd(&in_deg[r.dst], 1u);
+        if (undirected) {
+            rows[k + 1] = r.dst;
+            vals[k + 1] = bits | r.src;
+            atomicAdd(&out_deg[r.dst], 1u);
+            atomicAdd(&in_deg[r.src], 1u);
+        }
+    }
+}
+
+__global__ void split_values(const unsigned long long *__restrict__ vals, uint64_t m, uint32_t *nbr, float *data) {
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long v = vals[k];
+        nbr[k] = (uint32_t)v;
+        data[k] = __uint_as_float((uint32_t)(v >> 32));
+    }
+}
+
+// Loaded records to the device CSR, all on the device: validation, doubling,
+// a stable radix sort of the entries by source row (so each row keeps record
+// order, the reference's bucketing, graph.hpp:509-540), degrees, offsets,
+// then the acceptance thresholds.
 int build_graph(const HostEdge *edges, uint64_t n_edges, uint32_t v_num, int undirected, int device,
                 dg_graph **out) {
     DG_CHECK(out != nullptr, DG_ERR_ARG, "dg_graph_create: out is NULL");
@@ -81,47 +127,8 @@ int build_graph(const HostEdge *edges, uint64_t n_edges, uint32_t v_num, int und
     int n_dev = 0;
     DG_CUDA(cudaGetDeviceCount(&n_dev));
     DG_CHECK(device >= 0 && device < n_dev, DG_ERR_ARG, "dg_graph_create: device %d out of range (%d)", device, n_dev);
-    // Validate records the way the reference's asserts would fail (graph.hpp:639,
-    // walk.hpp:920 converts data to int).
-    for (uint64_t i = 0; i < n_edges; i++) {
-        const HostEdge &e = edges[i];
-        DG_CHECK(e.src < v_num && e.dst < v_num, DG_ERR_ARG,
-                 "edge %llu (%u, %u) has a vertex id >= v_num = %u", (unsigned long long)i, e.src, e.dst, v_num);
-        DG_CHECK(std::isfinite(e.data) && e.data > -2147483648.0f && e.data < 2147483648.0f, DG_ERR_ARG,
-                 "edge %llu has data %g outside the int range the transition converts it to",
-                 (unsigned long long)i, (double)e.data);
-    }
     const uint64_t m = undirected ? 2 * n_edges : n_edges;
     DG_CHECK(m < (1ull << 40), DG_ERR_ARG, "too many edges");
-
-    // CSR in record order (graph.hpp:671-686 doubling, 509-540 bucketing).
-    std::vector<uint32_t> out_deg(v_num, 0), in_deg(v_num, 0);
-    for (uint64_t i = 0; i < n_edges; i++) {
-        out_deg[edges[i].src]++;
-        in_deg[edges[i].dst]++;
-        if (undirected) {
-            out_deg[edges[i].dst]++;
-            in_deg[edges[i].src]++;
-        }
-    }
-    std::vector<uint64_t> offsets((size_t)v_num + 1, 0);
-    for (uint32_t v = 0; v < v_num; v++) offsets[v + 1] = offsets[v] + out_deg[v];
-    std::vector<uint32_t> nbr(m ? m : 1);
-    std::vector<float> data(m ? m : 1);
-    {
-        std::vector<uint64_t> cursor(offsets.begin(), offsets.end() - 1);
-        for (uint64_t i = 0; i < n_edges; i++) {
-            const HostEdge &e = edges[i];
-            uint64_t at = cursor[e.src]++;
-            nbr[at] = e.dst;
-            data[at] = e.data;
-            if (undirected) {
-                at = cursor[e.dst]++;
-                nbr[at] = e.src;
-                data[at] = e.data;
-            }
-        }
-    }
 
     dg::DeviceGuard guard(device);
     std::unique_ptr<dg_graph> g(new dg_graph());
@@ -129,34 +136,85 @@ int build_graph(const HostEdge *edges, uint64_t n_edges, uint32_t v_num, int und
     g->v_num = v_num;
     g->m = m;
     DG_CUDA(cudaStreamCreateWithFlags(&g->stream, cudaStreamNonBlocking));
+    cudaStream_t s = g->stream;
+    const unsigned grid = (unsigned)dg::sm_count(device) * 8;
     DG_CUDA(g->offsets.alloc((size_t)v_num + 1));
     DG_CUDA(g->entries.alloc(m));
     DG_CUDA(g->out_deg.alloc(v_num));
     DG_CUDA(g->in_deg.alloc(v_num));
     DG_CUDA(g->freq.alloc(v_num));
-    DG_CUDA(cudaMemcpyAsync(g->offsets.p, offsets.data(), offsets.size() * 8, cudaMemcpyHostToDevice, g->stream));
-    DG_CUDA(cudaMemcpyAsync(g->out_deg.p, out_deg.data(), (size_t)v_num * 4, cudaMemcpyHostToDevice, g->stream));
-    DG_CUDA(cudaMemcpyAsync(g->in_deg.p, in_deg.data(), (size_t)v_num * 4, cudaMemcpyHostToDevice, g->stream));
-    DG_CUDA(cudaMemsetAsync(g->freq.p, 0, (size_t)v_num * 4, g->stream));
-    if (m) {
-        dg::DevArray<uint32_t> d_nbr;
-        dg::DevArray<float> d_data;
-        DG_CUDA(d_nbr.alloc(m));
-        DG_CUDA(d_data.alloc(m));
-        DG_CUDA(cudaMemcpyAsync(d_nbr.p, nbr.data(), m * 4, cudaMemcpyHostToDevice, g->stream));
-        DG_CUDA(cudaMemcpyAsync(d_data.p, data.data(), m * 4, cudaMemcpyHostToDevice, g->stream));
-        dg::EventTimer t;
-        t.start(g->stream);
-        int blocks = dg::sm_count(device) * 8;
-        threshold_kernel<<<blocks, 256, 0, g->stream>>>(g->offsets.p, d_nbr.p, d_data.p, g->out_deg.p, v_num,
-                                                        g->entries.p); dg::note_launch();
+    DG_CUDA(cudaMemsetAsync(g->freq.p, 0, (size_t)v_num * 4, s));
+    DG_CUDA(cudaMemsetAsync(g->out_deg.p, 0, (size_t)v_num * 4, s));
+    DG_CUDA(cudaMemsetAsync(g->in_deg.p, 0, (size_t)v_num * 4, s));
+    if (n_edges) {
+        dg::DevArray<HostEdge> rec;
+        DG_CUDA(rec.alloc(n_edges));
+        DG_CUDA(cudaMemcpyAsync(rec.p, edges, n_edges * sizeof(HostEdge), cudaMemcpyHostToDevice, s));
+        dg::DevArray<unsigned long long> bad;
+        DG_CUDA(bad.alloc(1));
+        DG_CUDA(cudaMemsetAsync(bad.p, 0xFF, sizeof(unsigned long long), s));
+        check_records<<<grid, 256, 0, s>>>(rec.p, n_edges, v_num, bad.p);
+        dg::note_launch();
         DG_CUDA(cudaGetLastError());
-        t.stop(g->stream);
-        DG_CUDA(cudaStreamSynchronize(g->stream));
+        unsigned long long first_bad = 0;
+        DG_CUDA(cudaMemcpyAsync(&first_bad, bad.p, sizeof(first_bad), cudaMemcpyDeviceToHost, s));
+        DG_CUDA(cudaStreamSynchronize(s));
+        if (first_bad != ~0ull) {
+            const HostEdge &e = edges[first_bad];
+            if (!(e.src < v_num && e.dst < v_num))
+                return dg::fail(DG_ERR_ARG, "edge %llu (%u, %u) has a vertex id >= v_num = %u", first_bad, e.src,
+                                e.dst, v_num);
+            return dg::fail(DG_ERR_ARG, "edge %llu has data %g outside the int range the transition converts it to",
+                            first_bad, (double)e.data);
+        }
+        dg::DevArray<uint32_t> rows, rows_alt;
+        dg::DevArray<unsigned long long> vals, vals_alt;
+        DG_CUDA(rows.alloc(m));
+        DG_CUDA(vals.alloc(m));
+        emit_entries<<<grid, 256, 0, s>>>(rec.p, n_edges, undirected, rows.p, vals.p, g->out_deg.p, g->in_deg.p);
+        dg::note_launch();
+        DG_CUDA(cudaGetLastError());
+        DG_CUDA(cudaStreamSynchronize(s));
+        rec.release();
+        DG_CUDA(rows_alt.alloc(m));
+        DG_CUDA(vals_alt.alloc(m));
+        cub::DoubleBuffer<uint32_t> kb(rows.p, rows_alt.p);
+        cub::DoubleBuffer<unsigned long long> vb(vals.p, vals_alt.p);
+        const int end_bit = v_num > 1 ? 32 - __builtin_clz(v_num - 1) : 1;
+        {
+            size_t bytes = 0;
+            DG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kb, vb, m, 0, end_bit, s));
+            dg::DevArray<uint8_t> tmp;
+            DG_CUDA(tmp.alloc(bytes ? bytes : 1));
+            DG_CUDA(cub::DeviceRadixSort::SortPairs(tmp.p, bytes, kb, vb, m, 0, end_bit, s));
+            DG_CUDA(cudaStreamSynchronize(s));
+        }
+        if (vb.Current() != vals.p) vals.swap(vals_alt);
+        rows.release();
+        rows_alt.release();
+        // vals_alt (m x 8 bytes) holds the neighbour and data columns.
+        uint32_t *nbr = reinterpret_cast<uint32_t *>(vals_alt.p);
+        float *data = reinterpret_cast<float *>(vals_alt.p) + m;
+        split_values<<<grid, 256, 0, s>>>(vals.p, m, nbr, data);
+        dg::note_launch();
+        DG_CUDA(cudaGetLastError());
+        int rc = dg::exclusive_scan_u32_to_u64(g->out_deg.p, g->offsets.p, v_num, s);
+        if (rc) return rc;
+        vals.release();
+        dg::EventTimer t;
+        t.start(s);
+        threshold_kernel<<<grid, 256, 0, s>>>(g->offsets.p, nbr, data, g->out_deg.p, v_num, g->entries.p);
+        dg::note_launch();
+        DG_CUDA(cudaGetLastError());
+        t.stop(s);
+        DG_CUDA(cudaStreamSynchronize(s));
         g->threshold_ms = t.ms();
+    } else {
+        DG_CUDA(cudaMemsetAsync(g->offsets.p, 0, ((size_t)v_num + 1) * 8, s));
     }
-    DG_CUDA(cudaStreamSynchronize(g->stream));
-    g->h_out_deg.swap(out_deg);
+    g->h_out_deg.resize(v_num);
+    DG_CUDA(cudaMemcpyAsync(g->h_out_deg.data(), g->out_deg.p, (size_t)v_num * 4, cudaMemcpyDeviceToHost, s));
+    DG_CUDA(cudaStreamSynchronize(s));
     *out = g.release();
     return DG_OK;
 }

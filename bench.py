@@ -441,6 +441,64 @@ def run_auc_ours(args, local):
               flush=True)
 
 
+def run_gcn(args, local):
+    """Common-neighbour counts (the edge data the walk reads; the reference's gcn
+    tool, src/tools/gcn.cpp) on the YouTube-shaped graph, undirected: the device
+    kernel through the C ABI with host buffers in and out (copies timed), against
+    the reference tool compiled unmodified (oracle/_ref/gcn_ref) on all host cores
+    with the same edges as text.  One JSON line; `parity` compares every
+    (src, dst, count) triple of the two outputs."""
+    import numpy as np
+    import torch
+    from distger.synth import common_neighbours
+    torch.cuda.set_device(local)
+    edges = make_graph_edges()
+    v_num = graphgen_config()["n"]
+    src, dst = edges["src"], edges["dst"]
+    n = int(src.size)
+    common_neighbours(src, dst, v_num, device=local)   # warm-up: allocations, module load
+    times = []
+    for _ in range(max(args.steps, 1)):
+        t0 = time.perf_counter()
+        cn = common_neighbours(src, dst, v_num, device=local)
+        times.append(time.perf_counter() - t0)
+    t = statistics.median(times)
+    line = {"metric": "common-neighbour counts (gcn)", "unit": "edges/s", "impl": "ours", "value": n / t,
+            "ms_per_call": t * 1e3, "calls": len(times), "higher_is_better": True,
+            "config": {"graph": "youtube-shaped chung-lu", "vertices": v_num, "undirected_edges": n,
+                       "make_undirected": True, "buffers": "host in, host out (copies inside the timed call)"}}
+    import dgoracle
+    tool = os.path.join(dgoracle.HERE, "_ref", "gcn_ref")
+    if not os.path.exists(tool):
+        line["reference"] = {"unavailable": "oracle/_ref/gcn_ref not built (make -C oracle ref)"}
+    else:
+        import pandas as pd
+        cores = os.cpu_count() or 1
+        with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
+            inp, outp = os.path.join(tmp, "e.txt"), os.path.join(tmp, "o.txt")
+            pd.DataFrame({"s": src, "d": dst}).to_csv(inp, sep=" ", header=False, index=False)
+            t0 = time.perf_counter()
+            r = subprocess.run([tool, "-i", inp, "-o", outp, "-v", str(v_num), "-t", str(cores), "-s", "unweighted",
+                                "--make-undirected"], capture_output=True, text=True, timeout=args.ref_timeout)
+            tr = time.perf_counter() - t0
+            if r.returncode != 0:
+                line["reference"] = {"unavailable": f"gcn_ref exited {r.returncode}"}
+            else:
+                ref = pd.read_csv(outp, sep=" ", header=None).to_numpy(np.int64)
+                ours = np.stack([src.astype(np.int64), dst.astype(np.int64), cn.astype(np.int64)], axis=1)
+                same = ref.shape == ours.shape and np.array_equal(ref[np.lexsort(ref.T[::-1])],
+                                                                    ours[np.lexsort(ours.T[::-1])])
+                line["reference"] = {"value": n / tr, "unit": "edges/s", "cores": cores, "kind": "reference",
+                                     "seconds": tr, "note": "wall time of the tool: text read, counts, text write"}
+                line["parity"] = "identical (src, dst, count) triples on all edges" if same else "DIFFERS"
+    print(json.dumps(line))
+
+
+def graphgen_config():
+    from distger import graphgen
+    return graphgen.CONFIGS["c2_youtube"]
+
+
 def run_auc_reference(args):
     """The reference walk engine + dsgl (oracle/_ref/ref_embed) on the same split,
     all 30 rounds and the whole corpus, embedding scored by the same AUC code."""
@@ -597,6 +655,8 @@ def main():
                     help="graph of the --auc run (c5_twitter and *_device: generated and split on the device)")
     ap.add_argument("--rounds", type=int, default=30, help="--auc on device-generated graphs: walk rounds")
     ap.add_argument("--auc-modes", default="plain,minibatch")
+    ap.add_argument("--gcn", action="store_true",
+                    help="time the common-neighbour precompute against the reference gcn tool and exit")
     ap.add_argument("--plain-shape", type=int, default=None,
                     help="AUC runs: launch shape of the plain kernel (an index of the autotuner's list)")
     ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
@@ -607,6 +667,9 @@ def main():
     args = ap.parse_args()
     if args.profile:
         run_profile_case(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return
+    if args.gcn:
+        run_gcn(args, int(os.environ.get("LOCAL_RANK", "0")))
         return
     if args.auc:
         if args.impl == "reference":

@@ -45,7 +45,9 @@ WORKLOAD = {"graph": "youtube-shaped chung-lu", "vertices": 1_138_499, "undirect
             "exponent": 2.1, "max_degree": 28_000, "min_L": 20, "walkers_per_round": 1_138_499,
             "size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.01, "iter": 1,
             "min_count": 0}
-# Algorithmic bytes per unit (roofline section).
+# Algorithmic bytes per unit: plain SGNS pair = the context row and 1 + n output
+# rows, each read and written at 4 bytes; walk draw = 16 B row bounds + 4 B
+# neighbour + 4 B edge data + 4 B degree[dst], plus 4 B per footprint written.
 BYTES_PER_PAIR_PLAIN = lambda d, n: 2 * (2 + n) * d * 4          # noqa: E731  context + 1+n targets, read+write
 BYTES_PER_DRAW, BYTES_PER_FOOTPRINT = 28, 4
 BYTES_PER_ROW_MB = lambda d: 2 * d * 2                            # noqa: E731  BF16 row, read + write

@@ -625,9 +625,10 @@ def run_profile_case(args, local):
     p2 = eng.run_round(v_num, 3, n_walkers=args.profile_walks)
     out = {"case": args.profile, "walks": args.profile_walks, "walk_ms": p2.info.walk_ms,
            "draws": p2.info.draws, "footprints": p2.info.footprints}
-    if args.profile in ("sgns", "minibatch", "adjoint"):
+    if args.profile in ("sgns", "sgns_bf16", "minibatch", "adjoint"):
+        pmode = {"minibatch": "minibatch", "sgns_bf16": "plain_bf16"}.get(args.profile, "plain")
         s = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
-                 min_count=0, mode="minibatch" if args.profile == "minibatch" else "plain", seed=1,
+                 min_count=0, mode=pmode, seed=1,
                  deterministic=2 if args.profile == "adjoint" else 0, device=local)
         if args.profile == "sgns" and not args.no_autotune:
             # 7 shapes x 2 timed launches come first: profile with `ncu -s 14` to skip them.
@@ -642,7 +643,7 @@ def run_profile_case(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["walk", "sgns", "minibatch", "adjoint"], default=None,
+    ap.add_argument("--profile", choices=["walk", "sgns", "sgns_bf16", "minibatch", "adjoint"], default=None,
                     help="run one small launch of a kernel for ncu and exit")
     ap.add_argument("--profile-walks", type=int, default=50_000)
     ap.add_argument("--gpus", type=int, default=1)

@@ -549,32 +549,27 @@ struct BfRows {
             r.v[1] = __uint_as_float(t & 0xFFFF0000u);
         }
     }
-    // One hash per row write; each 32-bit word of noise rounds two elements, the
-    // next word comes from one LCG step.
+    // One hash per row write; each 32-bit word of noise rounds two elements (low
+    // half for the even element, high half for the odd one), the next word comes
+    // from one LCG step.  The rounding is bf16_sr_bits, done by the stochastic-
+    // rounding convert (cvt.rs.bf16x2.f32: upper result = a rounded with
+    // rbits[31:16], lower = b with rbits[15:0]), which gives bf16_sr_bits'
+    // result for every non-NaN input (infinities kept; a NaN stays a NaN).
     __device__ __forceinline__ void store_bits(int32_t w, uint32_t lane, const RowVec<VEC> &r, uint32_t salt) const {
-        uint16_t h[VEC];
+        uint32_t word[VEC / 2];
         uint32_t x = bf_mix(salt);
 #pragma unroll
         for (int i = 0; i < VEC; i += 2) {
-            h[i] = bf16_sr_bits(r.v[i], x);
-            h[i + 1] = bf16_sr_bits(r.v[i + 1], x >> 16);
+            asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(word[i / 2]) : "f"(r.v[i + 1]), "f"(r.v[i]), "r"(x));
             x = x * 0x9E3779B1u + 0x7F4A7C15u;
         }
         uint16_t *p = reinterpret_cast<uint16_t *>(bf + (size_t)w * d + lane * VEC);
         if constexpr (VEC == 8) {
-            uint4 t;
-            t.x = h[0] | ((uint32_t)h[1] << 16);
-            t.y = h[2] | ((uint32_t)h[3] << 16);
-            t.z = h[4] | ((uint32_t)h[5] << 16);
-            t.w = h[6] | ((uint32_t)h[7] << 16);
-            __stcg(reinterpret_cast<uint4 *>(p), t);
+            __stcg(reinterpret_cast<uint4 *>(p), make_uint4(word[0], word[1], word[2], word[3]));
         } else if constexpr (VEC == 4) {
-            uint2 t;
-            t.x = h[0] | ((uint32_t)h[1] << 16);
-            t.y = h[2] | ((uint32_t)h[3] << 16);
-            __stcg(reinterpret_cast<uint2 *>(p), t);
+            __stcg(reinterpret_cast<uint2 *>(p), make_uint2(word[0], word[1]));
         } else {
-            __stcg(reinterpret_cast<unsigned int *>(p), (unsigned int)(h[0] | ((uint32_t)h[1] << 16)));
+            __stcg(reinterpret_cast<unsigned int *>(p), word[0]);
         }
     }
     // Hogwild write of an updated row: FP32 masters (the hottest rows, where

@@ -853,6 +853,9 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
                     f[0] = s0;
                 }
                 uint32_t live = 0;
+                // BF16 rows: decoded once and kept for the update phase (FP32 rows
+                // are read from shared memory again instead, to save registers).
+                RowVec<VEC> kept[BF ? NS : 1];
 #pragma unroll
                 for (int j = 0; j < NS; j++) {
                     float sj = 0.f;
@@ -862,6 +865,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
 #pragma unroll
                         for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], r.v[i], sj);
                         if (t[j] != word) live |= 1u << j;
+                        if constexpr (BF) kept[j] = r;
                     }
                     f[j + 1] = sj;
                 }
@@ -883,7 +887,8 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
                 for (int j = 0; j < NS; j++) {
                     if (!((live >> j) & 1u)) continue;
                     RowVec<VEC> r, upd;
-                    read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], false, r);
+                    if constexpr (BF) r = kept[j];
+                    else read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], false, r);
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g[j + 1], r.v[i], e.v[i]);

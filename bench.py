@@ -41,10 +41,21 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "walk-steps/s + SGNS words/s, end-to-end embed time; BF16 vs FP32 plain at equal AUC"
 UNIT = "walk-steps/s"
-WORKLOAD = {"graph": "youtube-shaped chung-lu", "vertices": 1_138_499, "undirected_edges": 2_990_443,
-            "exponent": 2.1, "max_degree": 28_000, "min_L": 20, "walkers_per_round": 1_138_499,
-            "size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.01, "iter": 1,
-            "min_count": 0}
+SGNS_HP = {"size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.01, "iter": 1, "min_count": 0}
+# Bench workloads.  c5_twitter (the default): the Twitter-shaped graph, 41,652,230
+# vertices, Chung-Lu exponent 1.9, expected degrees capped at 3M, 2.417e9 edge draws
+# leaving ~1.47e9 unique undirected edges, unweighted; --min_R 5 (run.sh:45), walks
+# of at most 32 footprints; headline form: BF16 rows with FP32 masters (the plain
+# rule), FP32 plain beside it.  c2_youtube: the YouTube-shaped graph, FP32 plain.
+BENCH = {
+    "c5_twitter": dict(graph="twitter-shaped chung-lu, generated on the device", source="device",
+                       vertices=41_652_230, draws=2_417_000_000, exponent=1.9, max_degree=3_000_000, weighted=False,
+                       min_L=20, min_R=5, max_len=32, headline="plain_bf16", **SGNS_HP),
+    "c2_youtube": dict(graph="youtube-shaped chung-lu", source="host", vertices=1_138_499,
+                       undirected_edges=2_990_443, exponent=2.1, max_degree=28_000, weighted=True,
+                       min_L=20, min_R=10, max_len=64, headline="plain", **SGNS_HP),
+}
+WORKLOAD = dict(BENCH["c2_youtube"])   # the reference arm's C2 configuration
 # Algorithmic bytes per unit: plain SGNS pair = the context row and 1 + n output
 # rows, each read and written at 4 bytes; walk draw = 16 B row bounds + 4 B
 # neighbour + 4 B edge data + 4 B degree[dst], plus 4 B per footprint written.
@@ -145,8 +156,9 @@ def make_graph_edges():
     return graphgen.chung_lu(**graphgen.CONFIGS["c2_youtube"])
 
 
-def ref_baseline(edges_path: str, v_num: int, rounds: int, sgns_words: int, timeout: int = 900):
-    """Runs the reference walk engine + dsgl (oracle/_ref/ref_embed) on the host cores.
+def ref_baseline(edges_path: str, v_num: int, rounds: int, sgns_words: int, walkers: int = 0, timeout: int = 900):
+    """Runs the reference walk engine + dsgl (oracle/_ref/ref_embed) on the host cores,
+    `walkers` walkers per round (0: v_num) and round 1 with the same count.
     Returns per-round walk seconds, footprints, and dsgl words / seconds."""
     import dgoracle
     exe = os.path.join(dgoracle.HERE, "_ref", "ref_embed")
@@ -155,7 +167,7 @@ def ref_baseline(edges_path: str, v_num: int, rounds: int, sgns_words: int, time
     cores = os.cpu_count() or 1
     walk_threads = max(1, cores - 1)   # GraphEngine's worker_num = hw threads - 1 (graph.hpp:307)
     with tempfile.TemporaryDirectory() as tmp:
-        cmd = [exe, "-g", edges_path, "-v", str(v_num), "-w", str(v_num), "--min_L", "20", "--min_R", "1",
+        cmd = [exe, "-g", edges_path, "-v", str(v_num), "-w", str(walkers or v_num), "--min_L", "20", "--min_R", "1",
                "--make-undirected", "-t", str(walk_threads), "-o", os.path.join(tmp, "w"),
                "--walk-rounds", str(rounds), "--sgns-words", str(sgns_words), "-size", "128", "-window", "10",
                "-negative", "5", "-sample", "1e-3", "-alpha", "0.01", "-iter", "1", "-min-count", "0",
@@ -183,37 +195,135 @@ def pipeline_rate(walk_steps_per_s: float, words_per_s: float) -> float:
 
 
 def run_reference(args, rank, world, pg):
+    """The reference's own CPU implementation of the path (walk.hpp engine + dsgl,
+    oracle/_ref/ref_embed) on the host cores, on the bench workload: W + K walk
+    rounds of --ref-walkers walkers each (a prefix of the walker ids; walker w
+    starts at w % V, walk.hpp:501-509) and dsgl over the corpus of all those
+    rounds.  A step's time = its round's walk time (measured per round, without
+    the engine's dump and path assembly) + its share, by tokens, of dsgl's
+    measured time over the whole corpus; no time is extrapolated."""
     if rank != 0:
         return
-    edges = make_graph_edges()
+    wl = args.workload_bench
+    w = BENCH[wl]
+    form = args.mode or w["headline"]
     from distger import graphgen
-    with tempfile.TemporaryDirectory() as tmp:
+    with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
         path = os.path.join(tmp, "g.bin")
-        graphgen.write_edges(path, edges)
-        res = ref_baseline(path, 1_138_499, args.warmup + args.steps, args.ref_sgns_words)
+        if wl == "c5_twitter":
+            why = c5_reference_blocker(args.tmpdir)
+            if why:
+                print(json.dumps({"impl": "reference", "unavailable": why}))
+                return
+            write_c5_edges(path, int(os.environ.get("LOCAL_RANK", "0")))
+        else:
+            graphgen.write_edges(path, make_graph_edges())
+        res = ref_baseline(path, w["vertices"], args.warmup + args.steps, 0, walkers=args.ref_walkers,
+                           timeout=args.ref_timeout)
     if res is None or len(res["rounds"]) < args.warmup + args.steps or not res["sgns_train_s"]:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_embed missing or failed "
                           "(reference walk engine + dsgl built by make -C oracle ref)"}))
         return
+    all_fp = sum(r[1] for r in res["rounds"])
     timed = res["rounds"][args.warmup:]
+    fp = sum(r[1] for r in timed)
     walk_s = sum(r[0] for r in timed)
-    steps = sum(r[1] - r[2] for r in timed)
-    walk_rate = steps / walk_s
+    sgns_s = res["sgns_train_s"] * fp / all_fp
+    value = fp / (walk_s + sgns_s)
+    walk_rate = sum(r[1] - r[2] for r in timed) / walk_s
     word_rate = res["sgns_words"] / res["sgns_train_s"]
-    value = pipeline_rate(walk_rate, word_rate)
-    ms = 1e3 * sum(r[1] for r in timed) / value / len(timed)
-    sample = (f"C2 graph, {len(res['rounds'])} walk rounds of V walkers (walk.hpp internal_random_walk, "
-              f"{res['walk_threads']} threads), dsgl on the first {res['sgns_words']} corpus tokens "
-              f"({res['cores']} threads)")
+    sample = (f"{len(res['rounds'])} walk rounds of {args.ref_walkers} walkers on the same graph "
+              f"(walk.hpp internal_random_walk, {res['walk_threads']} threads), dsgl over their "
+              f"{res['sgns_words']} corpus tokens ({res['cores']} threads); first {args.warmup} rounds untimed")
+    cfg = {k: v for k, v in w.items() if k not in ("headline", "source")}
+    cfg.update(workload=f"{wl}_{form}", sgns_form=form, walkers_per_round=args.ref_walkers)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": dict(WORKLOAD, workload="c2_youtube_plain"),
-            "walk_steps_per_s": walk_rate, "sgns_words_per_s": word_rate,
+            "warmup": args.warmup, "ms_per_step": 1e3 * (walk_s + sgns_s) / len(timed), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": cfg, "walk_steps_per_s": walk_rate, "sgns_words_per_s": word_rate,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
+
+
+def host_memory_gb() -> float:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) / 1e6
+    except Exception:
+        pass
+    return 0.0
+
+
+# Host memory the reference's engine needs for the Twitter-shaped graph: the
+# records (12 B), their undirected doubling (2 x 12 B), the CSR it keeps
+# (8 B per directed entry) and its co-occurrence CSR (graph.hpp:376-472, about as
+# large again), plus the edge file written for it.
+C5_REF_HOST_GB = 1.47e9 * (12 + 24 + 16 + 16) / 1e9 + 60
+
+
+def c5_reference_blocker(tmpdir=None) -> str | None:
+    """Why the reference cannot run the Twitter-shaped graph on this host, or None."""
+    need = C5_REF_HOST_GB
+    have = host_memory_gb()
+    if have < need:
+        return (f"the reference walk engine needs about {need:.0f} GB of host memory for the Twitter-shaped graph "
+                f"(records, undirected doubling, CSR and co-occurrence CSR, graph.hpp:376-472, 642-824); "
+                f"this host has {have:.0f} GB available")
+    import shutil
+    free = shutil.disk_usage(tmpdir or tempfile.gettempdir()).free / 1e9
+    if free < 40:
+        return f"the Twitter-shaped edge file (17.6 GB) does not fit the {free:.0f} GB free in the temp directory"
+    return None
+
+
+def write_c5_edges(path: str, local: int) -> int:
+    """The Twitter-shaped graph's edges (the same device generator and seed as the
+    bench graph) as the reference's 12-byte records (storage.hpp:15-37)."""
+    import numpy as np
+    from distger import graphgen
+    from distger.synth import EdgeList
+    w = BENCH["c5_twitter"]
+    e = EdgeList.chung_lu(w["vertices"], w["draws"], w["exponent"], seed=0, max_degree=float(w["max_degree"]),
+                          weighted=w["weighted"], device=local)
+    src, dst, data = e.to_numpy()
+    e.close()
+    rec = np.empty(src.size, dtype=graphgen.EDGE_DTYPE)
+    rec["src"], rec["dst"], rec["data"] = src, dst, data
+    del src, dst, data
+    graphgen.write_edges(path, rec)
+    return int(rec.size)
+
+
+def cpu_baseline(args, wl, graph, host_edges):
+    """The reference's own walk engine + dsgl (oracle/_ref/ref_embed) on the box's
+    host cores, on a bounded sample of the same workload: one walk round of a
+    prefix of the walkers (walker ids 0.., starts id % V, walk.hpp:501-509) and
+    dsgl on the first --ref-sgns-words corpus tokens."""
+    from distger import graphgen
+    w = BENCH[wl]
+    with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
+        path = os.path.join(tmp, "g.bin")
+        if wl == "c5_twitter":
+            why = c5_reference_blocker(args.tmpdir)
+            if why:
+                return {"unavailable": why}
+            write_c5_edges(path, int(os.environ.get("LOCAL_RANK", "0")))
+            walkers = args.ref_walkers
+        else:
+            graphgen.write_edges(path, host_edges)
+            walkers = w["vertices"]
+        res = ref_baseline(path, w["vertices"], 1, args.ref_sgns_words, walkers=walkers, timeout=args.ref_timeout)
+    if not (res and res["rounds"] and res["sgns_train_s"]):
+        return {"unavailable": "oracle/_ref/ref_embed missing or failed"}
+    w_s, f_, n_ = res["rounds"][0]
+    cv = pipeline_rate((f_ - n_) / w_s, res["sgns_words"] / res["sgns_train_s"])
+    return {"value": cv, "unit": UNIT, "cores": res["cores"], "kind": "reference",
+            "sample": f"one walk round of {walkers} walkers on the same graph ({res['walk_threads']} threads) + "
+                      f"dsgl on {res['sgns_words']} tokens ({res['cores']} threads)",
+            "walk_steps_per_s": (f_ - n_) / w_s, "sgns_words_per_s": res["sgns_words"] / res["sgns_train_s"]}
 
 
 def load_traffic():
@@ -224,39 +334,70 @@ def load_traffic():
         return {}
 
 
-def run_ours(args, rank, world, local, pg):
-    import numpy as np
-    import torch
+def build_bench_graph(workload: str, local: int):
+    """The workload's graph as a device CSR.  c5_twitter: generated, deduplicated and
+    built on the device (dg_edges_chung_lu, dg_graph_create_from_device_edges);
+    c2_youtube: the numpy generator's records loaded through dg_graph_create_from_edges.
+    Returns (graph, edge info, CSR build ms, host edges or None)."""
     import distger
+    w = BENCH[workload]
+    if w["source"] == "device":
+        from distger.synth import EdgeList
+        e = EdgeList.chung_lu(w["vertices"], w["draws"], w["exponent"], seed=0, max_degree=float(w["max_degree"]),
+                              weighted=w["weighted"], device=local)
+        n_edges = e.n
+        torch_sync(local)
+        t0 = time.perf_counter()
+        graph = e.graph()
+        torch_sync(local)
+        build_ms = (time.perf_counter() - t0) * 1e3
+        e.close()
+        return graph, {"undirected_edges": n_edges}, build_ms, None
+    edges = make_graph_edges()
+    distger.Graph(w["vertices"], edges=edges, make_undirected=True, device=local).close()   # context, module load
+    t0 = time.perf_counter()
+    graph = distger.Graph(w["vertices"], edges=edges, make_undirected=True, device=local)
+    build_ms = (time.perf_counter() - t0) * 1e3   # host records -> device CSR with thresholds
+    return graph, {"records": int(edges.size)}, build_ms, edges
+
+
+def torch_sync(local: int):
+    import torch
+    torch.cuda.synchronize(local)
+
+
+def sgns_kernel_name(form: str) -> str:
+    return {"plain": "sgns_plain", "plain_bf16": "sgns_plain_bf16", "minibatch": "sgns_minibatch",
+            "cbow": "sgns_cbow", "sg_shared": "sgns_sg_shared"}[form]
+
+
+def measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=False):
+    """Warm-up and timed pipeline steps (one walk round of V walkers streamed into
+    SGNS, dg_pipeline_round) of one trainer form; returns its counters, the trainer
+    and the walk parameters."""
+    import torch
     from distger import _lib
     from distger._lib import check, lib
     from distger.sgns import SGNS
-
-    torch.cuda.set_device(local)
     L = lib()
-    edges = make_graph_edges()
-    v_num = 1_138_499
-    distger.Graph(v_num, edges=edges, make_undirected=True, device=local).close()   # context and module load
-    t_graph = time.perf_counter()
-    graph = distger.Graph(v_num, edges=edges, make_undirected=True, device=local)
-    graph_build_ms = (time.perf_counter() - t_graph) * 1e3   # host records -> device CSR with thresholds
-    csr = graph.csr()
-    counts = csr["out_deg"] + csr["in_deg"]              # word2vec vocabulary from degrees (huge_walk.cpp:43-46)
-    mode = args.mode
-    sgns = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
-                min_count=0, mode=mode, seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local)
-    form = mode + ("_adjoint" if args.adjoint else "")
-    wp = _lib.WalkParams(min_len=20, init_round=10, walker_num=v_num, max_len=64, seed=2024 + rank)
+    w = BENCH[wl]
+    v_num = w["vertices"]
+    sgns = SGNS(v_num, counts, size=w["size"], window=w["window"], negative=w["negative"], batch_size=21,
+                sample=w["sample"], alpha=w["alpha"], iter=w["iter"], min_count=w["min_count"], mode=form,
+                seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local)
+    wp = _lib.WalkParams(min_len=w["min_L"], init_round=w["min_R"], walker_num=v_num, max_len=w["max_len"],
+                         seed=2024 + rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
-
-    # Launch shapes timed on this workload before anything is measured (dg_walk_autotune, dg_sgns_autotune).
+    # Launch shapes timed on this workload before anything is measured (dg_walk_autotune,
+    # dg_sgns_autotune), on at most 2M walkers of a round so that tuning stays short.
     tune = {}
     if not args.no_autotune:
+        n_tune = min(v_num, 2_000_000)
         ti = _lib.TuneInfo()
-        check(L.dg_walk_autotune(graph.handle, C.byref(wp), 2, v_num, C.byref(ti)))
+        check(L.dg_walk_autotune(graph.handle, C.byref(wp), 2, n_tune, C.byref(ti)))
         tune["walk"] = ti.as_dict()
         ph = C.c_void_p()
-        check(L.dg_walk_run_round(graph.handle, C.byref(wp), 90, v_num, C.byref(ph)))
+        check(L.dg_walk_run_round(graph.handle, C.byref(wp), 90, n_tune, C.byref(ph)))
         ti = _lib.TuneInfo()
         check(L.dg_sgns_autotune(sgns.handle, ph, C.byref(ti)))
         tune["sgns"] = ti.as_dict()
@@ -270,40 +411,51 @@ def run_ours(args, rank, world, local, pg):
 
     for i in range(args.warmup):
         step(2 + i)
-    clocks = Clocks(local) if rank == 0 else None
+    clocks = Clocks(local) if (with_clocks and rank == 0) else None
     if clocks:
         clocks.start()
     barrier(pg)
     torch.cuda.synchronize()
     l0 = L.dg_launch_count()
-    tot_ms = walk_ms = train_ms = 0.0
-    fp = steps_ = draws = words = pairs = rows = 0
+    acc = dict(tot_ms=0.0, walk_ms=0.0, train_ms=0.0, fp=0, steps=0, draws=0, words=0, pairs=0, rows=0)
     for k in range(args.steps):
         flush.zero_()
         torch.cuda.synchronize()
         info = step(2 + args.warmup + k)
-        tot_ms += info.total_ms
-        walk_ms += info.walk.walk_ms
-        train_ms += info.train.train_ms
-        fp += info.walk.footprints
-        steps_ += info.walk.steps
-        draws += info.walk.draws
-        words += info.train.words
-        pairs += info.train.pairs
-        rows += info.train.rows
+        acc["tot_ms"] += info.total_ms
+        acc["walk_ms"] += info.walk.walk_ms
+        acc["train_ms"] += info.train.train_ms
+        acc["fp"] += info.walk.footprints
+        acc["steps"] += info.walk.steps
+        acc["draws"] += info.walk.draws
+        acc["words"] += info.train.words
+        acc["pairs"] += info.train.pairs
+        acc["rows"] += info.train.rows
     torch.cuda.synchronize()
     barrier(pg)
-    launches = L.dg_launch_count() - l0
-    clk = clocks.stop() if clocks else None
+    acc["launches"] = L.dg_launch_count() - l0
+    acc["clocks"] = clocks.stop() if clocks else None
+    acc["tune"] = tune
+    t_dev = reduce_max(pg, acc["tot_ms"] / 1e3)
+    acc["t_dev"] = t_dev
+    acc["value"] = reduce_sum(pg, acc["fp"]) / t_dev
+    del flush
+    return acc, sgns, wp
 
-    # e2e: the reference-facing calls with host buffers (pinned), copies timed.
+
+def measure_e2e(args, graph, sgns, wp, v_num, max_len, pg):
+    """The same step through the reference-facing calls with host buffers: walks
+    copied to pinned host memory (dg_paths_copy) and trained from there
+    (dg_sgns_train_host), both copies inside the timed region."""
+    import torch
+    from distger import _lib
+    from distger._lib import check, lib
+    L = lib()
     n_walks = v_num
-    cap = n_walks * 64
     h_off = torch.empty(n_walks + 1, dtype=torch.int64, pin_memory=True)
-    h_verts = torch.empty(cap, dtype=torch.int32, pin_memory=True)
+    h_verts = torch.empty(n_walks * max_len, dtype=torch.int32, pin_memory=True)
     e2e_s = 0.0
-    e2e_fp = 0
-    h2d = d2h = 0
+    e2e_fp = h2d = d2h = 0
     for k in range(args.steps + 1):
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -324,78 +476,119 @@ def run_ours(args, rank, world, local, pg):
         e2e_fp += ri.footprints
         d2h += (n_walks + 1) * 8 + ri.footprints * 4 + 32
         h2d += (n_walks + 1) * 8 + ri.footprints * 4
-    t_dev = reduce_max(pg, tot_ms / 1e3)
-    all_fp = reduce_sum(pg, fp)
-    value = all_fp / t_dev
-    e2e_t = reduce_max(pg, e2e_s)
-    e2e_value = reduce_sum(pg, e2e_fp) / e2e_t
+    del h_off, h_verts
+    return reduce_sum(pg, e2e_fp) / reduce_max(pg, e2e_s), h2d / args.steps, d2h / args.steps
 
-    # Roofline of the dominant kernel.
+
+def roofline(wl, form, acc, args):
+    """Roofline of the dominant kernel.  achieved = the DRAM bytes the kernel moves
+    per launch (ncu dram__bytes per unit measured on this workload, profiles/traffic.json,
+    times the launch's units) / its CUDA-event time, so frac is the share of the
+    measured copy bandwidth the kernel uses; l2_plus_dram_frac uses the access
+    model's bytes instead (every row access counted, L2 hits included)."""
     hbm, peak_kind = peaks()
-    traffic = load_traffic()
-    if train_ms >= walk_ms:
-        kern = "sgns_plain" if mode == "plain" else "sgns_minibatch"
-        # minibatch form: every step reads and writes its I input and O output rows
-        # at 2 bytes (the FP32 master rows counted at 2 bytes too)
-        alg = pairs * BYTES_PER_PAIR_PLAIN(128, 5) if mode == "plain" else rows * BYTES_PER_ROW_MB(128)
-        if mode == "plain_bf16":
-            # rows at 2 bytes (the 65,536 FP32 master rows are counted at 2 bytes too)
-            kern, alg = "sgns_plain_bf16", pairs * BYTES_PER_PAIR_PLAIN(128, 5) / 2
+    traffic = load_traffic().get(wl, {})
+    w = BENCH[wl]
+    d, n = w["size"], w["negative"]
+    if acc["train_ms"] >= acc["walk_ms"]:
+        kern = sgns_kernel_name(form)
+        e = 2 if form in ("plain_bf16", "minibatch") else 4
+        if form == "minibatch":
+            model = acc["rows"] * 2 * d * e
+        elif form == "cbow":
+            model = None
+        elif form == "sg_shared":
+            model = acc["pairs"] * 2 * d * e
+        else:
+            model = acc["pairs"] * 2 * (2 + n) * d * e
         if args.adjoint:
-            kern = "sgns_adjoint pass (pair cut + gradient + step kernels)"
-            alg = pairs * BYTES_PER_PAIR_ADJOINT(128, 5, 21, 4 if mode == "plain" else 2)
-        kms = train_ms
-        per = traffic.get(kern, {}).get("dram_bytes_per_pair")
-        tr = per * pairs / args.steps if per else None
-        per_word = traffic.get(kern, {}).get("dram_bytes_per_word")
-        if per_word:
-            tr = per_word * words / args.steps
+            kern = "sgns_adjoint"
+            model = acc["pairs"] * BYTES_PER_PAIR_ADJOINT(d, n, 21, 4 if form == "plain" else 2)
+        kms = acc["train_ms"]
+        t = traffic.get(kern, {})
+        measured = None
+        if t.get("dram_bytes_per_pair"):
+            measured = t["dram_bytes_per_pair"] * acc["pairs"]
+        elif t.get("dram_bytes_per_word"):
+            measured = t["dram_bytes_per_word"] * acc["words"]
     else:
         kern = "walk"
-        alg = draws * BYTES_PER_DRAW + fp * BYTES_PER_FOOTPRINT
-        kms = walk_ms
-        per = traffic.get("walk", {}).get("dram_bytes_per_draw")
-        tr = per * draws / args.steps if per else None
-    roof = None
-    if alg is not None:
-        achieved = alg / (kms / 1e3) / 1e9
-        roof = {"kernel": kern, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": tr,
-                "algorithmic_bytes_per_launch": alg / args.steps}
+        model = acc["draws"] * BYTES_PER_DRAW + acc["fp"] * BYTES_PER_FOOTPRINT
+        kms = acc["walk_ms"]
+        t = traffic.get("walk", {})
+        measured = t["dram_bytes_per_draw"] * acc["draws"] if t.get("dram_bytes_per_draw") else None
+    sec = kms / 1e3
+    per_launch = lambda x: None if x is None else x / args.steps   # noqa: E731
+    roof = {"kernel": kern, "bound": "hbm", "peak": hbm, "unit": "GB/s", "peak_kind": peak_kind,
+            "traffic": per_launch(measured), "traffic_source": t.get("source"),
+            "model_bytes_per_launch": per_launch(model)}
+    if measured is not None:
+        roof["achieved"] = measured / sec / 1e9
+        roof["basis"] = "measured DRAM bytes per unit (ncu) x units / kernel time"
+    elif model is not None:
+        roof["achieved"] = model / sec / 1e9
+        roof["basis"] = "access-model bytes (L2 hits included) / kernel time"
+    else:
+        roof["achieved"] = None
+    roof["frac"] = roof["achieved"] / hbm if roof["achieved"] else None
+    if model is not None:
+        roof["l2_plus_dram_frac"] = model / sec / 1e9 / hbm
+    # The measured bytes of the whole step cannot outrun the copy bandwidth.
+    roof["bound_check"] = "ok" if measured is None or measured / (acc["t_dev"] or 1) / 1e9 <= hbm * 1.02 \
+        else "measured bytes / step time exceeds the copy bandwidth"
+    return roof
+
+
+def run_ours(args, rank, world, local, pg):
+    import torch
+    from distger import _lib
+
+    torch.cuda.set_device(local)
+    wl = args.workload_bench
+    w = BENCH[wl]
+    v_num = w["vertices"]
+    form = args.mode or w["headline"]
+    graph, einfo, graph_build_ms, host_edges = build_bench_graph(wl, local)
+    out_deg, in_deg = graph.degrees()
+    counts = out_deg + in_deg              # word2vec vocabulary from degrees (huge_walk.cpp:43-46)
+
+    acc, sgns, wp = measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=True)
+    e2e_value, h2d, d2h = measure_e2e(args, graph, sgns, wp, v_num, w["max_len"], pg)
+    sgns.close()
+    roof = roofline(wl, form, acc, args)
+    # FP32 plain (word2vec.cu's skip_gram_kernel rule) on the same graph, beside the headline form.
+    plain = None
+    if form != "plain" and not args.no_plain_leg:
+        pacc, psgns, _ = measure_form(args, "plain", graph, counts, wl, rank, local, pg)
+        psgns.close()
+        plain = {"value": pacc["value"], "unit": UNIT, "ms_per_step": pacc["t_dev"] * 1e3 / args.steps,
+                 "walk_steps_per_s": pacc["steps"] / (pacc["walk_ms"] / 1e3),
+                 "sgns_words_per_s": pacc["words"] / (pacc["train_ms"] / 1e3),
+                 "sgns_ms_per_step": pacc["train_ms"] / args.steps, "dtype": "f32",
+                 "roofline": roofline(wl, "plain", pacc, args)}
 
     line = None
     if rank == 0:
         cpu = None
         if world == 1 and not args.no_cpu_baseline:
-            from distger import graphgen
-            with tempfile.TemporaryDirectory() as tmp:
-                path = os.path.join(tmp, "g.bin")
-                graphgen.write_edges(path, edges)
-                res = ref_baseline(path, v_num, 1, args.ref_sgns_words)
-            if res and res["rounds"] and res["sgns_train_s"]:
-                w_s, f_, n_ = res["rounds"][0]
-                cv = pipeline_rate((f_ - n_) / w_s, res["sgns_words"] / res["sgns_train_s"])
-                cpu = {"value": cv, "unit": UNIT, "cores": res["cores"], "kind": "reference",
-                       "sample": f"one walk round of V walkers on the same graph ({res['walk_threads']} threads) + "
-                                 f"dsgl on {res['sgns_words']} tokens ({res['cores']} threads)",
-                       "walk_steps_per_s": (f_ - n_) / w_s,
-                       "sgns_words_per_s": res["sgns_words"] / res["sgns_train_s"]}
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": t_dev * 1e3 / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if mode == "plain" else "bf16",
-                "data": "synthetic",
-                "config": dict(WORKLOAD, workload="c2_youtube_" + form,
-                               sgns_form=form, l2="flushed between steps (256 MB write)",
-                               parallelism=f"replicas x{world}"),
-                "walk_steps_per_s": steps_ / (walk_ms / 1e3), "sgns_words_per_s": words / (train_ms / 1e3),
-                "walk_ms_per_step": walk_ms / args.steps, "sgns_ms_per_step": train_ms / args.steps,
-                "footprints_per_step": fp / args.steps, "pairs_per_step": pairs / args.steps,
+            cpu = cpu_baseline(args, wl, graph, host_edges)
+        cfg = {k: v for k, v in w.items() if k not in ("headline", "source")}
+        cfg.update(einfo)
+        cfg.update(workload=f"{wl}_{form}" + ("_adjoint" if args.adjoint else ""), sgns_form=form,
+                   walkers_per_round=v_num, l2="flushed between steps (256 MB write); rows and CSR exceed L2",
+                   parallelism=f"replicas x{world}")
+        line = {"metric": METRIC, "value": acc["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": acc["t_dev"] * 1e3 / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if form in ("plain", "cbow", "sg_shared") else "bf16",
+                "data": "synthetic", "config": cfg,
+                "walk_steps_per_s": acc["steps"] / (acc["walk_ms"] / 1e3),
+                "sgns_words_per_s": acc["words"] / (acc["train_ms"] / 1e3),
+                "walk_ms_per_step": acc["walk_ms"] / args.steps, "sgns_ms_per_step": acc["train_ms"] / args.steps,
+                "footprints_per_step": acc["fp"] / args.steps, "pairs_per_step": acc["pairs"] / args.steps,
                 "graph_build_ms": graph_build_ms,
-                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d / args.steps,
-                        "d2h_bytes_per_step": d2h / args.steps},
-                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
-                "autotune": tune}
-    sgns.close()
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+                "gpu_launches": acc["launches"], "clocks": acc["clocks"], "roofline": roof, "cpu_baseline": cpu,
+                "fp32_plain": plain, "autotune": acc["tune"]}
     graph.close()
     return line
 
@@ -650,11 +843,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["plain", "plain_bf16", "minibatch"], default="plain")
+    ap.add_argument("--mode", choices=["plain", "plain_bf16", "minibatch", "cbow", "sg_shared"], default=None,
+                    help="trainer form of the bench line (default: the workload's headline form)")
+    ap.add_argument("--bench-workload", dest="workload_bench", choices=sorted(BENCH), default="c5_twitter")
+    ap.add_argument("--no-plain-leg", action="store_true", help="skip the FP32 plain measurement beside the headline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
+    ap.add_argument("--ref-walkers", type=int, default=100_000,
+                    help="walkers of each of the reference's sampled walk rounds (a prefix of the walker ids)")
     ap.add_argument("--auc", action="store_true",
                     help="run the whole embedding job on a 10%%-held-out split and print link-prediction AUC lines")
     ap.add_argument("--workload", choices=["c1_small", "c2_youtube", "c3_livejournal", "c5_twitter",

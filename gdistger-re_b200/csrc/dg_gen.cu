@@ -587,7 +587,7 @@ extern "C" int dg_lp_auc(const dg_sgns *s, const dg_lp_pairs *t, double *auc, do
     dg::DevArray<uint64_t> sig, cosk;
     DG_CUDA(sig.alloc(n));
     DG_CUDA(cosk.alloc(n));
-    const bool plain = s->p.mode == DG_SGNS_PLAIN;
+    const bool plain = dgs::fp32_rows(s);
     const unsigned grid = (unsigned)dg::sm_count(s->device) * 8;
     switch (s->p.size) {
 #define DG_LP_CASE(V)                                                                                        \

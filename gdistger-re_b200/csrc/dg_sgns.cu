@@ -7,6 +7,7 @@
 //  * minibatch form (DG_SGNS_MINIBATCH): dsgl.hpp Train_SGNS_MPI semantics
 //    (dsgl.hpp:783-1407), see dg_sgns_mb.cu.
 #include "dg_sgns.h"
+#include "dg_sgns_dev.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -111,9 +112,16 @@ __device__ __forceinline__ unsigned long long lcg_state(unsigned long long k) {
     return ra * 1ULL + rc;
 }
 
-__global__ void init_rows_f32(float *rows, uint64_t n, int d) {
+// Row r, column c < d gets element r * d + c of word2vec's sequence (rows of d
+// columns); rows are stored with stride dp >= d and the padding columns are 0.
+__global__ void init_rows_f32(float *rows, uint64_t n, int d, int dp) {
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
-        const unsigned long long x = lcg_state(k);
+        const uint64_t r = k / (uint64_t)dp, c = k % (uint64_t)dp;
+        if (c >= (uint64_t)d) {
+            rows[k] = 0.f;
+            continue;
+        }
+        const unsigned long long x = lcg_state(r * (uint64_t)d + c);
         rows[k] = (((x & 0xFFFF) / (float)65536) - 0.5f) / d;
     }
 }
@@ -128,118 +136,6 @@ __global__ void init_rows_bf16(__nv_bfloat16 *rows, float *master, uint64_t n, u
 }
 
 // ------------------------------------------------------------ plain kernel
-
-template <int VEC>
-struct RowVec {
-    float v[VEC];
-};
-
-template <int VEC>
-__device__ __forceinline__ void load_row(const float *p, RowVec<VEC> &r) {
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4) {
-            const float4 t = __ldcg(reinterpret_cast<const float4 *>(p + i));
-            r.v[i] = t.x; r.v[i + 1] = t.y; r.v[i + 2] = t.z; r.v[i + 3] = t.w;
-        }
-    } else if constexpr (VEC == 2) {
-        const float2 t = __ldcg(reinterpret_cast<const float2 *>(p));
-        r.v[0] = t.x; r.v[1] = t.y;
-    } else {
-        r.v[0] = __ldcg(p);
-    }
-}
-
-template <int VEC>
-__device__ __forceinline__ void store_row(float *p, const RowVec<VEC> &r) {
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4)
-            __stcg(reinterpret_cast<float4 *>(p + i), make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]));
-    } else if constexpr (VEC == 2) {
-        __stcg(reinterpret_cast<float2 *>(p), make_float2(r.v[0], r.v[1]));
-    } else {
-        __stcg(p, r.v[0]);
-    }
-}
-
-// p[i] += r[i] with 16-byte vector atomics (sm_90+).
-template <int VEC>
-__device__ __forceinline__ void add_row(float *p, const RowVec<VEC> &r) {
-    if constexpr (VEC % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < VEC; i += 4)
-            atomicAdd(reinterpret_cast<float4 *>(p + i), make_float4(r.v[i], r.v[i + 1], r.v[i + 2], r.v[i + 3]));
-    } else if constexpr (VEC == 2) {
-        atomicAdd(reinterpret_cast<float2 *>(p), make_float2(r.v[0], r.v[1]));
-    } else {
-        atomicAdd(p, r.v[0]);
-    }
-}
-
-template <int VEC>
-__device__ __forceinline__ float warp_dot(const RowVec<VEC> &a, const RowVec<VEC> &b) {
-    float s = 0.f;
-#pragma unroll
-    for (int i = 0; i < VEC; i++) s = fmaf(a.v[i], b.v[i], s);
-    // Butterfly: lanes i and i^o add the same two values (in swapped order, which
-    // float addition does not see), so every lane ends with the same sum.
-#pragma unroll
-    for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-    return s;
-}
-
-
-// g = (label - sigmoid(f)) * alpha through expTable (word2vec.cu:383-388), with
-// the reference's integer-division index scale (EXP_TABLE_SIZE / MAX_EXP / 2 = 83).
-__device__ __forceinline__ float sg_grad(float f, int label, const float *exp_table, float alpha) {
-    if (f > kMaxExp) return (label - 1) * alpha;
-    if (f < -kMaxExp) return label * alpha;
-    return (label - __ldg(exp_table + (int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2)))) * alpha;
-}
-
-// Brings [p, p + bytes) into L2 (bytes a multiple of 16, p 16-byte aligned).  A
-// hint only: it holds no registers and orders nothing.
-__device__ __forceinline__ void prefetch_l2(const void *p, uint32_t bytes) {
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(__cvta_generic_to_global(p)), "r"(bytes));
-}
-
-__device__ __forceinline__ uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0, uint32_t k1) {
-    return philox4x32_10(make_uint4(c0, c1, c2, c3), k0, k1);
-}
-
-// Builds the walk's sentence in shared memory: vocabulary lookup + subsampling
-// (word2vec.cu:1011-1029 with a Philox draw in place of rand()).  Returns its length.
-// At most CAP tokens of a walk are used.
-template <uint32_t CAP = kMaxSentence>
-__device__ __forceinline__ uint32_t warp_sentence(const WalkSet &ws, uint32_t walk, const SgnsArgs &a, int32_t *sen,
-                                                  uint32_t &words) {
-    const uint32_t lane = threadIdx.x & 31;
-    uint64_t begin;
-    uint32_t len;
-    ws.range(walk, begin, len);
-    if (len > CAP) len = CAP;
-    words = len;
-    uint32_t n = 0;
-    for (uint32_t base = 0; base < len; base += 32) {
-        const uint32_t i = base + lane;
-        bool keep = false;
-        int32_t w = -1;
-        if (i < len) {
-            w = a.v2w[ws.verts[begin + i]];
-            if (w >= 0) {
-                const uint32_t u = philox(i, ws.ids ? ws.ids[walk] : walk + ws.id_base, a.pass, kSubTag, a.seed_lo,
-                                          a.seed_hi).x & 0xFFFFu;
-                keep = u < a.keep_thr[w];
-            }
-        }
-        const uint32_t mask = __ballot_sync(0xffffffffu, keep);
-        if (keep) sen[n + __popc(mask & ((1u << lane) - 1))] = w;
-        n += __popc(mask);
-    }
-    __syncwarp();
-    return n;
-}
 
 // Negative target j (1-based) of pair (centre p, window slot s) of walk wid:
 // unigram table draw with word2vec's replacement of index 0 (word2vec.cu:365-368).
@@ -422,7 +318,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g[0], l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
 #pragma unroll
                     for (int j = 0; j < NS; j++) {
@@ -448,7 +344,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g, pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g, l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
                 }
 #pragma unroll
@@ -881,7 +777,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
 #pragma unroll
                 for (int i = 0; i < VEC; i++) {
                     e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
-                    pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                    pos.v[i] += __fmul_rn(g[0], l1.v[i]);  // rounded product, as the reference's atomicAdd
                 }
 #pragma unroll
                 for (int j = 0; j < NS; j++) {
@@ -903,7 +799,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g, pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g, l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
                 }
                 uint32_t f32 = 0;   // bit k: slot k was rewritten with FP32 values
@@ -1061,7 +957,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g[0], pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g[0], l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g[0], l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
 #pragma unroll
                     for (int j = 0; j < NS; j++) {
@@ -1083,7 +979,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_bf16_ke
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g, pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g, l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
                 }
 #pragma unroll
@@ -1174,7 +1070,7 @@ __global__ void __launch_bounds__(kPlainThreads) sgns_plain_seq_kernel(SgnsArgs 
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
                         e.v[i] = fmaf(g, pos.v[i], e.v[i]);
-                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
+                        pos.v[i] += __fmul_rn(g, l1.v[i]);  // rounded product, as the reference's atomicAdd
                     }
                 }
                 if (a.vocab_size > 1) {
@@ -1517,10 +1413,16 @@ __global__ void rows_from_f32(const float *in, uint64_t n, uint64_t n_master, __
     }
 }
 
+bool fp32_rows(const dg_sgns *s) {
+    return s->p.mode == DG_SGNS_PLAIN || s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_SG_SHARED;
+}
+
 int copy_rows(const dg_sgns *s, bool input, float *host) {
     const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
-    if (s->p.mode == DG_SGNS_PLAIN) {
-        DG_CUDA(cudaMemcpyAsync(host, input ? s->syn0.p : s->syn1.p, n * 4, cudaMemcpyDeviceToHost, s->stream));
+    if (fp32_rows(s)) {
+        // Rows of out_size columns from rows stored with stride p.size.
+        DG_CUDA(cudaMemcpy2DAsync(host, (size_t)s->out_size * 4, input ? s->syn0.p : s->syn1.p, (size_t)s->p.size * 4,
+                                  (size_t)s->out_size * 4, s->vocab_size, cudaMemcpyDeviceToHost, s->stream));
         DG_CUDA(cudaStreamSynchronize(s->stream));
         return DG_OK;
     }
@@ -1556,12 +1458,24 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CHECK(p && vertex_counts && out, DG_ERR_ARG, "dg_sgns_create: NULL argument");
     *out = nullptr;
     DG_CHECK(v_num > 0, DG_ERR_ARG, "dg_sgns_create: v_num must be positive");
-    DG_CHECK(p->size >= 32 && p->size <= 512 && p->size % 32 == 0 && ((p->size / 32) & (p->size / 32 - 1)) == 0,
-             DG_ERR_ARG, "size %d not supported (32, 64, 128, 256 or 512)", p->size);
+    const bool fp32_mode = p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED;
+    const bool pow2_size =
+        p->size >= 32 && p->size <= 512 && p->size % 32 == 0 && ((p->size / 32) & (p->size / 32 - 1)) == 0;
+    DG_CHECK(pow2_size || (fp32_mode && p->deterministic != 2 && p->size >= 1 && p->size <= 512), DG_ERR_ARG,
+             "size %d not supported (32, 64, 128, 256 or 512; the FP32 word2vec rules also take any size up to 512, "
+             "except in adjoint mode)", p->size);
     DG_CHECK(p->window >= 1 && p->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", p->window);
     DG_CHECK(p->negative >= 0 && p->negative <= 64, DG_ERR_ARG, "negative %d out of range [0, 64]", p->negative);
-    DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH || p->mode == DG_SGNS_PLAIN_BF16, DG_ERR_ARG,
-             "unknown mode %d", p->mode);
+    DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH || p->mode == DG_SGNS_PLAIN_BF16 ||
+                 p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED,
+             DG_ERR_ARG, "unknown mode %d", p->mode);
+    DG_CHECK(p->mode != DG_SGNS_CBOW || p->negative <= kCbowMaxNeg, DG_ERR_ARG, "the CBOW trainer supports negative <= %d",
+             kCbowMaxNeg);
+    DG_CHECK(p->mode != DG_SGNS_SG_SHARED || p->negative <= kShareMaxNeg, DG_ERR_ARG,
+             "the shared-negative trainer supports negative <= %d", kShareMaxNeg);
+    DG_CHECK(p->deterministic != 2 || p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH ||
+                 p->mode == DG_SGNS_PLAIN_BF16,
+             DG_ERR_ARG, "adjoint mode trains the skip-gram rules only");
     DG_CHECK(p->mode != DG_SGNS_PLAIN_BF16 || ((p->size == 64 || p->size == 128 || p->size == 256) && p->negative <= 8),
              DG_ERR_ARG, "the BF16 plain trainer supports size 64, 128 or 256 and negative <= 8");
     DG_CHECK(p->iter >= 1, DG_ERR_ARG, "iter must be >= 1");
@@ -1574,6 +1488,15 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     std::unique_ptr<dg_sgns> s(new dg_sgns());
     s->device = device;
     s->p = *p;
+    // FP32 rules: rows of any size are stored padded to the next of 32 .. 512
+    // columns (zeros that no update changes: every update of a padding column
+    // adds g * 0), so the kernels see one of their sizes.
+    s->out_size = p->size;
+    if (fp32_mode) {
+        int dp = 32;
+        while (dp < p->size) dp *= 2;
+        s->p.size = dp;
+    }
     if (s->p.table_size == 0) s->p.table_size = kDefaultTableSize;
     DG_CHECK(s->p.table_size < (1ull << 32), DG_ERR_ARG, "table_size must be < 2^32");
     s->v_num = v_num;
@@ -1602,12 +1525,12 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CUDA(cudaMemcpyAsync(s->keep_thr.p, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, s->stream));
     DG_CUDA(cudaMemcpyAsync(s->table.p, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s->stream));
     DG_CUDA(cudaMemcpyAsync(s->exp_table.p, et.data(), et.size() * 4, cudaMemcpyHostToDevice, s->stream));
-    const uint64_t n = (uint64_t)s->vocab_size * p->size;
+    const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
     const int blocks = dg::sm_count(device) * 8;
-    if (p->mode == DG_SGNS_PLAIN) {
+    if (p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED) {
         DG_CUDA(s->syn0.alloc(n));
         DG_CUDA(s->syn1.alloc(n));
-        init_rows_f32<<<blocks, 256, 0, s->stream>>>(s->syn0.p, n, p->size); dg::note_launch();
+        init_rows_f32<<<blocks, 256, 0, s->stream>>>(s->syn0.p, n, s->out_size, s->p.size); dg::note_launch();
         DG_CUDA(cudaGetLastError());
         DG_CUDA(cudaMemsetAsync(s->syn1.p, 0, n * 4, s->stream));
     } else {
@@ -1671,7 +1594,10 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
             rc = adjoint_train(s, a, ws, np);
             adj_pairs += np;
         } else {
-            rc = s->p.mode == DG_SGNS_MINIBATCH ? launch_minibatch(s, a, ws) : launch_plain(s, a, ws);
+            rc = s->p.mode == DG_SGNS_MINIBATCH   ? launch_minibatch(s, a, ws)
+                 : s->p.mode == DG_SGNS_CBOW      ? launch_cbow(s, a, ws)
+                 : s->p.mode == DG_SGNS_SG_SHARED ? launch_negshare(s, a, ws)
+                                                  : launch_plain(s, a, ws);
         }
         if (rc) return rc;
     }
@@ -1701,7 +1627,8 @@ extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alph
 extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info *info) {
     DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_autotune: NULL argument");
     dg_tune_info r{};
-    if (s->p.mode == DG_SGNS_MINIBATCH || s->p.deterministic || s->p.negative > dgs::kFastNeg) {
+    if (s->p.mode == DG_SGNS_MINIBATCH || s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_SG_SHARED ||
+        s->p.deterministic || s->p.negative > dgs::kFastNeg) {
         r.n_candidates = 1;
         r.chosen = 0;
         if (info) *info = r;
@@ -1912,8 +1839,10 @@ extern "C" int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float
     for (int k = 0; k < 2; k++) {
         const float *src = k == 0 ? input_rows : output_rows;
         if (!src) continue;
-        if (s->p.mode == DG_SGNS_PLAIN) {
-            DG_CUDA(cudaMemcpyAsync(k == 0 ? s->syn0.p : s->syn1.p, src, n * 4, cudaMemcpyHostToDevice, s->stream));
+        if (dgs::fp32_rows(s)) {
+            DG_CUDA(cudaMemcpy2DAsync(k == 0 ? s->syn0.p : s->syn1.p, (size_t)s->p.size * 4, src,
+                                      (size_t)s->out_size * 4, (size_t)s->out_size * 4, s->vocab_size,
+                                      cudaMemcpyHostToDevice, s->stream));
         } else {
             dg::DevArray<float> tmp;
             DG_CUDA(tmp.alloc(n));
@@ -1935,7 +1864,7 @@ extern "C" int dg_sgns_set_rows(dg_sgns *s, const float *input_rows, const float
 extern "C" int dg_sgns_write_embedding(const dg_sgns *s, const char *file_path) {
     DG_CHECK(s && file_path, DG_ERR_ARG, "dg_sgns_write_embedding: NULL argument");
     const uint32_t rows = s->vocab_size;
-    const int d = s->p.size;
+    const int d = s->out_size;
     std::vector<float> emb((size_t)rows * d);
     dg::DeviceGuard guard(s->device);
     int rc = dgs::copy_rows(s, true, emb.data());

@@ -36,6 +36,8 @@ constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 i
 constexpr uint32_t kSubTag = 0x53554253u;  // subsampling of token i
 constexpr uint32_t kWinTag = 0x57494E44u;  // window shrink of centre p
 constexpr uint32_t kNegTag = 0x4E454730u;  // negatives of pair (p, slot), + j / 4
+constexpr uint32_t kCbowTag = 0x43424F57u;   // CBOW negatives of centre p, + j / 4
+constexpr uint32_t kShareTag = 0x53484E47u;  // shared negatives of a walk (counter word 0 = 0), + j / 4
 
 // Walks to train on: slot layout (verts + w * stride, lens[w]) or compact
 // (verts + offsets[w] .. offsets[w + 1]).
@@ -111,6 +113,11 @@ constexpr int pow2_at_least(int x) { return x <= 1 ? 1 : 2 * pow2_at_least((x + 
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 bool bf_staging_safe(const std::vector<uint32_t> &cn, uint32_t n_master, int negative, int sms);
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+// cbow_kernel and __sgNegReuse semantics (dg_sgns_w2v.cu).
+int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+int launch_negshare(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+constexpr int kCbowMaxNeg = 32;   // one negative per lane
+constexpr int kShareMaxNeg = 16;  // shared negatives held in shared memory per warp
 
 // Concurrency bound of the minibatch form from the vocabulary (counts in
 // vocabulary order, subsampling keep thresholds out of 65536).
@@ -139,10 +146,18 @@ struct AdjStep {
 
 }  // namespace dgs
 
+struct dg_sgns;
+namespace dgs {
+// Whether the trainer keeps its rows in FP32 (syn0 / syn1): the word2vec.cu
+// rules; the minibatch and BF16 forms keep BF16 rows + FP32 masters.
+bool fp32_rows(const dg_sgns *s);
+}  // namespace dgs
+
 struct dg_sgns {
     int device = 0;
     cudaStream_t stream = nullptr;
-    dg_sgns_params p{};
+    dg_sgns_params p{};                // p.size: the row stride the kernels use (padded for the FP32 rules)
+    int out_size = 0;                  // the caller's -size: columns of the embedding
     uint32_t v_num = 0;
     uint32_t vocab_size = 0;
     uint32_t n_master = 0;

@@ -382,7 +382,7 @@ AdjArgs adjoint_args(dg_sgns *s, const uint32_t *inputs, const uint32_t *outputs
     a.step = nullptr;
     a.batch = batch;
     a.negative = negative;
-    const bool plain = s->p.mode == DG_SGNS_PLAIN;
+    const bool plain = dgs::fp32_rows(s);
     a.in_f32 = plain ? s->syn0.p : nullptr;
     a.out_f32 = plain ? s->syn1.p : nullptr;
     a.in_bf = s->in_bf.p;
@@ -541,7 +541,7 @@ int adjoint_train(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
             cudaGraphExecDestroy(s->adj_exec);
             s->adj_exec = nullptr;
         }
-        const bool plain = s->p.mode == DG_SGNS_PLAIN;
+        const bool plain = dgs::fp32_rows(s);
         AdjArgs ga = adjoint_args(s, s->adj_pin.p, s->adj_pout.p, s->adj_neg.p, 0, batch, neg);
         ga.step = s->adj_step.p;
         AdjLaunch l;
@@ -584,6 +584,8 @@ int adjoint_train(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws, uint64_t &n_
 extern "C" int dg_sgns_loss_grad(dg_sgns *s, const dg_sgns_pairs *pairs, double *loss, float *grad_in,
                                  float *grad_out) {
     DG_CHECK(s, DG_ERR_ARG, "dg_sgns_loss_grad: NULL trainer");
+    DG_CHECK(s->out_size == s->p.size, DG_ERR_ARG, "dg_sgns_loss_grad: size %d is stored padded; use 32 .. 512, "
+             "a power of two", s->out_size);
     dg::DeviceGuard guard(s->device);
     int rc = dgs::adjoint_run(s, pairs, loss);
     if (rc) return rc;
@@ -606,12 +608,14 @@ extern "C" int dg_sgns_loss_grad(dg_sgns *s, const dg_sgns_pairs *pairs, double 
 
 extern "C" int dg_sgns_adjoint_step(dg_sgns *s, const dg_sgns_pairs *pairs, float alpha, double *loss) {
     DG_CHECK(s, DG_ERR_ARG, "dg_sgns_adjoint_step: NULL trainer");
+    DG_CHECK(s->out_size == s->p.size, DG_ERR_ARG, "dg_sgns_adjoint_step: size %d is stored padded; use 32 .. 512, "
+             "a power of two", s->out_size);
     DG_CHECK(std::isfinite(alpha), DG_ERR_ARG, "alpha must be finite");
     dg::DeviceGuard guard(s->device);
     int rc = dgs::adjoint_run(s, pairs, loss);
     if (rc) return rc;
     const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
-    const bool plain = s->p.mode == DG_SGNS_PLAIN;
+    const bool plain = dgs::fp32_rows(s);
     const uint64_t nm = plain ? 0 : (uint64_t)s->n_master * s->p.size;
     for (int k = 0; k < 2; k++) {
         dgs::adjoint_apply<<<dg::sm_count(s->device) * 4, 256, 0, s->stream>>>(

@@ -743,9 +743,10 @@ int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 // Allocation-free entry point: the minibatch trainer with its per-worker
 // scratch (negative pools and cache snapshots) in a fixed device array that is
 // part of this library, so that a call performs no device or host allocation.
-// It serves callers that must not allocate: code running inside a CUDA graph
-// capture, a memory pool owned by a framework that forbids foreign cudaMalloc,
-// or a real-time loop that cannot pay an allocator's latency or failure modes.
+// It serves callers that must not allocate: a host framework whose memory pool
+// owns the device memory and forbids foreign cudaMalloc, or a latency-bound loop
+// that cannot pay cudaMalloc / cudaFree (which can synchronise the device) or
+// handle an allocation failure in the middle of training.
 // ---------------------------------------------------------------------------
 namespace dgs {
 namespace {
@@ -803,6 +804,16 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
     if (rc) return rc;
     int device = 0;
     DG_CUDA(cudaGetDevice(&device));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (s) {
+        // The scratch address and the worker count are those of the current
+        // device, so the stream must belong to it.
+        int stream_device = -1;
+        DG_CUDA(cudaStreamGetDevice(s, &stream_device));
+        DG_CHECK(stream_device == device, DG_ERR_ARG,
+                 "dg_sgns_minibatch_train_noalloc: the stream belongs to device %d but device %d is current",
+                 stream_device, device);
+    }
     float *scratch = nullptr;
     unsigned long long *stats = nullptr;
     rc = noalloc_pointers(device, &scratch, &stats);
@@ -814,7 +825,10 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
              d, x->negative, (unsigned long long)per_worker, kNoAllocScratchBytes);
     uint64_t workers = x->deterministic ? 1 : (uint64_t)dg::sm_count(device) * plan.per_sm;
     workers = std::min<uint64_t>(workers, max_workers);
-    if (!x->deterministic && x->workers) workers = std::min<uint64_t>(workers, x->workers);
+    // workers = 0: kMbMaxHolders workers, the staleness bound that holds whatever
+    // the vocabulary (even if every worker held the hottest row); the handle
+    // path's bound for a given vocabulary is what dg_sgns_get_info reports.
+    if (!x->deterministic) workers = std::min<uint64_t>(workers, x->workers ? x->workers : (uint64_t)kMbMaxHolders);
     if (workers > x->n_walks / 2 + 1) workers = std::max<uint64_t>(1, x->n_walks / 2);
 
     SgnsArgs a{};
@@ -845,7 +859,6 @@ extern "C" int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *x, 
     MbArgs m = plan.m;
     m.scratch = scratch;
 
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     DG_CUDA(cudaMemsetAsync(stats, 0, 4 * sizeof(unsigned long long), s));  // counters start at zero every call
     mb_launch(d, (unsigned)workers, plan, s, a, ws, m);
     DG_CUDA(cudaGetLastError());

@@ -1,0 +1,369 @@
+// The two other negative-sampling trainers of word2vec.cu, on FP32 rows over
+// device-resident walks, one warp per walk (lane l owns columns
+// [l*VEC, l*VEC+VEC) of every row):
+//
+//  * DG_SGNS_CBOW: cbow_kernel (word2vec.cu:401-509), the reference's default
+//    trainer (cbow = 1, word2vec.cu:59).  Per centre: the mean of the shrunk
+//    window's context rows, one positive and `negative` sampled targets, their
+//    gradient e added to every context row.
+//  * DG_SGNS_SG_SHARED: __sgNegReuse (word2vec.cu:231-303), the reference's
+//    skip-gram when -cbow 0 (reuseNeg = 1): one negative set per sentence, the
+//    full window, the centre's output row as the positive, the context row
+//    updated by the pair's e.  The reference instantiates it for size 200 and
+//    300 only and exits for others (word2vec.cu:914-926); here every size the
+//    trainer supports runs it.  Its dot products are warp sums (the reference's
+//    reduceInWarp adds a fixed lane's value at each step, not the partner's).
+//
+// Per-pair arithmetic is the reference's: cbow e += g*syn1 fused, syn1 +=
+// rounded g*neu1; shared-negative e += rounded g*syn1, syn1 += g*l1 fused.
+// deterministic = 1: one warp, walks in order, plain loads and stores (bit-
+// exact against oracle/dg_oracle_w2v.c's device form).  Hogwild: many warps,
+// vector atomics for row updates.
+#include "dg_sgns.h"
+#include "dg_sgns_dev.cuh"
+
+#include <algorithm>
+
+namespace dgs {
+
+constexpr int kW2vThreads = 256;
+
+// Negative j (0-based) drawn from (c0, walk, pass, tag + j/4), word j%4, with
+// word2vec's replacement of index 0 (word2vec.cu:365-368).
+__device__ __forceinline__ int32_t tagged_negative(const SgnsArgs &a, uint32_t c0, uint32_t wid, uint32_t tag, int j) {
+    const uint4 blk = philox(c0, wid, a.pass, tag + (uint32_t)(j >> 2), a.seed_lo, a.seed_hi);
+    const uint32_t q = j & 3;
+    const uint32_t r = q == 0 ? blk.x : q == 1 ? blk.y : q == 2 ? blk.z : blk.w;
+    int32_t t = a.table[r % a.table_size];
+    if (t == 0) t = (int32_t)((r >> 8) % (a.vocab_size - 1) + 1);
+    return t;
+}
+
+template <int VEC>
+__device__ __forceinline__ void zero_row(RowVec<VEC> &r) {
+#pragma unroll
+    for (int i = 0; i < VEC; i++) r.v[i] = 0.f;
+}
+
+// ------------------------------------------------------------------ CBOW
+
+// G: target rows fetched together (their loads overlap); later groups are
+// fetched after the earlier ones are written.
+template <int VEC, int G>
+__global__ void __launch_bounds__(kW2vThreads) sgns_cbow_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31;
+    int32_t *sen = sen_all[threadIdx.x >> 5];
+    const int d = 32 * VEC;
+    const uint32_t w = (uint32_t)a.window;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
+            const uint32_t lo = max(b, w > p ? w - p : 0u), hi = min(2 * w + 1 - b, n + w - p);
+            const uint32_t cw = hi > lo ? hi - lo - ((lo <= w && w < hi) ? 1u : 0u) : 0u;
+            if (cw == 0) continue;
+            n_pairs += cw;
+            // neu1: context rows summed in window order (word2vec.cu:419-428), four
+            // rows in flight at a time, then divided by their count.
+            RowVec<VEC> neu1;
+            zero_row(neu1);
+            for (uint32_t s = lo; s < hi; s += 4) {
+                RowVec<VEC> r[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (s + k < hi && s + k != w)
+                        load_row<VEC>(a.syn0 + (size_t)sen[p - w + s + k] * d + lane * VEC, r[k]);
+#pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (s + k < hi && s + k != w) {
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) neu1.v[i] = neu1.v[i] + r[k].v[i];
+                    }
+            }
+#pragma unroll
+            for (int i = 0; i < VEC; i++) neu1.v[i] = __fdiv_rn(neu1.v[i], (float)cw);
+            // Targets: the centre, then the negatives that differ from it
+            // (word2vec.cu:453-462); lane j draws negative j.
+            int32_t mine = -1;
+            if (a.vocab_size > 1 && (int)lane < a.negative)
+                mine = tagged_negative(a, p, wid, kCbowTag, (int)lane);
+            const int nt = 1 + (a.vocab_size > 1 ? a.negative : 0);
+            RowVec<VEC> e;
+            zero_row(e);
+            for (int g0 = 0; g0 < nt; g0 += G) {
+                int32_t t[G];
+                RowVec<VEC> row[G];
+#pragma unroll
+                for (int k = 0; k < G; k++) {
+                    const int j = g0 + k;
+                    t[k] = j >= nt ? -1 : j == 0 ? word : __shfl_sync(0xffffffffu, mine, (j - 1) & 31);
+                    if (j > 0 && t[k] == word) t[k] = -1;
+                    if (t[k] >= 0) load_row<VEC>(a.syn1 + (size_t)t[k] * d + lane * VEC, row[k]);
+                }
+#pragma unroll
+                for (int k = 0; k < G; k++) {
+                    if (t[k] < 0) continue;
+                    const float g = sg_grad(warp_dot<VEC>(neu1, row[k]), g0 + k == 0, a.exp_table, a.alpha);
+                    RowVec<VEC> upd;
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, row[k].v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, neu1.v[i]);
+                        row[k].v[i] += upd.v[i];
+                    }
+                    float *rp = a.syn1 + (size_t)t[k] * d + lane * VEC;
+                    if (a.deterministic) store_row<VEC>(rp, row[k]);
+                    else add_row<VEC>(rp, upd);
+                    // A repeat of this target later in the group sees this update.
+#pragma unroll
+                    for (int q = k + 1; q < G; q++)
+                        if (t[q] == t[k]) row[q] = row[k];
+                }
+            }
+            // e to every context row, in window order (word2vec.cu:498-505).
+            for (uint32_t s = lo; s < hi; s++) {
+                if (s == w) continue;
+                float *cp = a.syn0 + (size_t)sen[p - w + s] * d + lane * VEC;
+                if (a.deterministic) {
+                    RowVec<VEC> r;
+                    load_row<VEC>(cp, r);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) r.v[i] = r.v[i] + e.v[i];
+                    store_row<VEC>(cp, r);
+                } else {
+                    add_row<VEC>(cp, e);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
+// ------------------------------------------------ shared-negative skip-gram
+
+// The walk's negative rows live in the warp's shared memory for the duration of
+// one centre (loaded at its start, written back at its end: stored in
+// deterministic mode, their change added atomically otherwise), so the up to
+// 2 * window pairs of a centre read and update them there; the centre's output
+// row (the positive) stays in registers, or is the shared copy when the centre
+// word is one of the negatives.  Shared memory per warp: the sentence, the
+// negatives, and 2 x negative rows (current and as loaded).
+template <int VEC>
+__global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, WalkSet ws) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int d = 32 * VEC;
+    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    const size_t warp_bytes = (size_t)kMaxSentence * 4 + kShareMaxNeg * 8 + (size_t)2 * neg * d * 4;
+    unsigned char *base = smem_raw + warp * warp_bytes;
+    int32_t *sen = reinterpret_cast<int32_t *>(base);
+    int32_t *negs = reinterpret_cast<int32_t *>(base + (size_t)kMaxSentence * 4);
+    int32_t *slot = negs + kShareMaxNeg;  // slot of negative j: index of its first occurrence
+    float *cur = reinterpret_cast<float *>(base + (size_t)kMaxSentence * 4 + kShareMaxNeg * 8);
+    float *init = cur + (size_t)neg * d;
+    const uint32_t w = (uint32_t)a.window;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        if (n < 2) continue;
+        if ((int)lane < neg) negs[lane] = tagged_negative(a, 0, wid, kShareTag, (int)lane);
+        __syncwarp();
+        if ((int)lane < neg) {
+            int s = (int)lane;
+            for (int k = 0; k < (int)lane; k++)
+                if (negs[k] == negs[lane]) { s = k; break; }
+            slot[lane] = s;
+        }
+        __syncwarp();
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            // This centre's rows: the distinct negatives into shared memory, the
+            // positive into registers unless it is one of them.
+            int pslot = -1;
+            for (int j = 0; j < neg; j++) {
+                if (slot[j] != j) continue;
+                if (negs[j] == word) pslot = j;
+                RowVec<VEC> r;
+                load_row<VEC>(a.syn1 + (size_t)negs[j] * d + lane * VEC, r);
+#pragma unroll
+                for (int i = 0; i < VEC; i++) cur[(size_t)j * d + lane * VEC + i] = init[(size_t)j * d + lane * VEC + i] = r.v[i];
+            }
+            RowVec<VEC> pos, pos0;
+            if (pslot < 0) {
+                load_row<VEC>(a.syn1 + (size_t)word * d + lane * VEC, pos);
+                pos0 = pos;
+            }
+            const uint32_t lo = w > p ? w - p : 0u, hi = min(2 * w + 1, n + w - p);
+            for (uint32_t s = lo; s < hi; s++) {
+                if (s == w) continue;
+                n_pairs++;
+                float *l1p = a.syn0 + (size_t)sen[p - w + s] * d + lane * VEC;
+                RowVec<VEC> l1, e;
+                load_row<VEC>(l1p, l1);
+                zero_row(e);
+                // Negatives in order (those equal to the centre skipped), then the
+                // positive (word2vec.cu:256-297; the reference's warps y < negative,
+                // then y = negative).
+                for (int j = 0; j <= neg; j++) {
+                    float *sr = nullptr;
+                    if (j < neg) {
+                        if (negs[j] == word) continue;
+                        sr = cur + (size_t)slot[j] * d + lane * VEC;
+                    } else if (pslot >= 0) {
+                        sr = cur + (size_t)pslot * d + lane * VEC;
+                    }
+                    RowVec<VEC> r;
+                    if (sr) {
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) r.v[i] = sr[i];
+                    } else {
+                        r = pos;
+                    }
+                    const float g = sg_grad(warp_dot<VEC>(l1, r), j == neg, a.exp_table, a.alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] += __fmul_rn(g, r.v[i]);
+                        r.v[i] = fmaf(g, l1.v[i], r.v[i]);
+                    }
+                    if (sr) {
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) sr[i] = r.v[i];
+                    } else {
+                        pos = r;
+                    }
+                }
+                if (a.deterministic) {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) l1.v[i] = l1.v[i] + e.v[i];
+                    store_row<VEC>(l1p, l1);
+                } else {
+                    add_row<VEC>(l1p, e);
+                }
+            }
+            // Write the centre's rows back.
+            for (int j = 0; j < neg; j++) {
+                if (slot[j] != j) continue;
+                float *dst = a.syn1 + (size_t)negs[j] * d + lane * VEC;
+                RowVec<VEC> r;
+#pragma unroll
+                for (int i = 0; i < VEC; i++) {
+                    const float c = cur[(size_t)j * d + lane * VEC + i];
+                    r.v[i] = a.deterministic ? c : c - init[(size_t)j * d + lane * VEC + i];
+                }
+                if (a.deterministic) store_row<VEC>(dst, r);
+                else add_row<VEC>(dst, r);
+            }
+            if (pslot < 0) {
+                float *dst = a.syn1 + (size_t)word * d + lane * VEC;
+                if (a.deterministic) {
+                    store_row<VEC>(dst, pos);
+                } else {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
+                    add_row<VEC>(dst, pos);
+                }
+            }
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
+// --------------------------------------------------------------- launchers
+
+template <typename K>
+static int resident_blocks(K kern, int threads, size_t smem, int device) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    return std::max(per_sm, 1) * dg::sm_count(device);
+}
+
+static int worker_blocks(const dg_sgns *s, int resident, int threads) {
+    if (s->p.workers == 0) return resident;
+    const int want = (int)((s->p.workers + threads / 32 - 1) / (threads / 32));
+    return std::max(1, std::min(resident, want));
+}
+
+template <int V>
+static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    constexpr int G = V <= 4 ? 6 : 2;
+    auto kern = sgns_cbow_kernel<V, G>;
+    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
+    kern<<<blocks, threads, 0, s->stream>>>(a, ws);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
+size_t negshare_warp_bytes(int negative, int size) {
+    return (size_t)kMaxSentence * 4 + kShareMaxNeg * 8 + (size_t)2 * negative * size * 4;
+}
+
+template <int V>
+static int negshare_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    auto kern = sgns_negshare_kernel<V>;
+    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    const size_t per_warp = negshare_warp_bytes(neg, s->p.size);
+    // As many warps per block (up to 8) as fit in 200 KB of shared memory.
+    const int warps = s->p.deterministic ? 1 : (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / per_warp));
+    const int threads = 32 * warps;
+    const size_t smem = per_warp * warps;
+    DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, smem, s->device), threads);
+    kern<<<blocks, threads, smem, s->stream>>>(a, ws);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
+int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    switch (s->p.size / 32) {
+        case 1: return cbow_launch<1>(s, a, ws);
+        case 2: return cbow_launch<2>(s, a, ws);
+        case 4: return cbow_launch<4>(s, a, ws);
+        case 8: return cbow_launch<8>(s, a, ws);
+        case 16: return cbow_launch<16>(s, a, ws);
+        default: return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
+    }
+}
+
+int launch_negshare(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    switch (s->p.size / 32) {
+        case 1: return negshare_launch<1>(s, a, ws);
+        case 2: return negshare_launch<2>(s, a, ws);
+        case 4: return negshare_launch<4>(s, a, ws);
+        case 8: return negshare_launch<8>(s, a, ws);
+        case 16: return negshare_launch<16>(s, a, ws);
+        default: return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
+    }
+}
+
+}  // namespace dgs

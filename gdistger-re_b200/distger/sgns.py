@@ -4,7 +4,9 @@
 word2vec.cu:1545-1565) and dsgl (dsgl.hpp:1497-1548): size, window, negative,
 batch_size, sample, alpha, iter, min_count.  mode="plain" follows word2vec.cu's
 skip_gram_kernel update rule on FP32 rows; mode="minibatch" follows dsgl's
-shared-negative minibatches on BF16 rows.  The learning-rate schedules of
+shared-negative minibatches on BF16 rows; mode="cbow" follows cbow_kernel (the
+reference's default, -cbow 1) and mode="sg_shared" __sgNegReuse (-cbow 0
+-reuse-neg 1: one negative set per walk, full window), both on FP32 rows.  The learning-rate schedules of
 include/lr_scheduler.hpp are restated below for the per-round loop.
 """
 from __future__ import annotations
@@ -17,7 +19,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 
-MODES = {"plain": 0, "minibatch": 1, "plain_bf16": 2}
+MODES = {"plain": 0, "minibatch": 1, "plain_bf16": 2, "cbow": 3, "sg_shared": 4}
 
 
 class SGNS:

@@ -6,26 +6,34 @@
 // vertices' in+out degrees (huge_walk.cpp:40-44, word2vec.cu:791-809), then run
 // the walk rounds of WalkEngine::random_walk (walk.hpp:609-782: round 1 with
 // -w x --min_R walkers, then -w walkers per round, 30 rounds) and stream every
-// round's walks straight into the trainer with the round's learning rate from
-// the schedule (word2vec.cu:1279-1290 uses ExponentialDecayLR(alpha, 0.1)).  The
-// reference writes each round to ./out/tmp-0-<r>.txt and reads it back; here the
-// walks stay in HBM and are written only when -o is given.
+// trained round's walks straight into the trainer with the round's learning
+// rate from the schedule.  The reference writes each round to
+// ./out/tmp-0-<r>.txt and trains on files 3..30 (word2vec.cu:1285-1296), with
+// alpha = ExponentialDecayLR(0.025, 0.1).get_lr() per file (word2vec.cu:1279-1290:
+// the schedule overrides -alpha and the -cbow default of 0.05); here the walks
+// stay in HBM and are written only when -o is given, and those are the defaults.
 //
-// Flags kept from the reference (option_helper.hpp:112-156, word2vec.cu:1546-1563,
+// Flags kept from the reference (option_helper.hpp:112-156, word2vec.cu:1546-1565,
 // dsgl.hpp:1496-1535):
 //   -g <edges.bin> -v <vertices> -w <walkers> [-o <walk prefix>] [--min_L n]
 //   [--min_R n] [--make-undirected] [-r rate: accepted, unused as in walk.hpp:616]
 //   -size -window -negative -batch-size -sample -alpha -iter -min-count
 //   -emb_output <file> (word2vec.cu) or -eoutput <file> (dsgl)
-//   -threads / -debug / -reuse-neg: accepted, no effect on one GPU
-//   -hs, -cbow, -binary: only 0 is supported (skip-gram, negative sampling, text)
+//   -cbow 0|1 (default 1, word2vec.cu:59): cbow_kernel; -cbow 0 selects skip-gram,
+//     with -reuse-neg 1 (default, word2vec.cu:59) __sgNegReuse's shared
+//     negatives, with -reuse-neg 0 skip_gram_kernel (word2vec.cu:1073-1076, 912)
+//   -threads / -debug / -sync-size / -sync-period ...: accepted, no effect on one GPU
+//   -hs, -binary: only 0 is supported (negative sampling, text output)
 // Added for the GPU build:
-//   -mode plain|plain_bf16|minibatch   trainer form (default plain = word2vec.cu semantics
-//                           on FP32 rows; plain_bf16: the same rule on BF16 rows)
+//   -mode plain|plain_bf16|minibatch|cbow|sg_shared   trainer form, overriding -cbow /
+//                           -reuse-neg (plain = skip_gram_kernel on FP32 rows;
+//                           plain_bf16: the same rule on BF16 rows; minibatch: dsgl)
 //   -lr exp|fixed|cosine|step|custom   per-round schedule (default exp, decay 0.1)
+//   -lr-start a             the schedule's first rate (default 0.025, word2vec.cu:1279;
+//                           -alpha does not change it, as in the reference)
 //   -rounds n               stop after round n (default 30)
-//   -train-from n           first round whose walks are trained (default 1;
-//                           word2vec.cu:1286 starts at round 3)
+//   -train-from n           first round whose walks are trained (default 3,
+//                           word2vec.cu:1286)
 //   -seed s  -device d  -master-rows n  -table-size n  -max-len n
 //   -deterministic 0|1|2    0 Hogwild, 1 one worker in order, 2 adjoint gradient steps
 //   -workers n              concurrent trainer workers (0 = automatic)
@@ -46,13 +54,14 @@
 namespace {
 
 struct Options {
-    std::string graph, walk_prefix, emb_output, mode = "plain", lr = "exp";
+    std::string graph, walk_prefix, emb_output, mode, lr = "exp";
     uint32_t v_num = 0, walker_num = 0, min_len = 0, init_round = 0;
     bool undirected = false;
     int size = 100, window = 5, negative = 5, batch_size = 11, iter = 5, min_count = 5;
-    float sample = 1e-3f, alpha = 0.025f;
+    float sample = 1e-3f, alpha = 0.025f, lr_start = 0.025f;
     bool alpha_set = false;
-    int rounds = 30, train_from = 1, device = 0, deterministic = 0, max_len = 0;
+    int cbow = 1, reuse_neg = 1;  // word2vec.cu:59
+    int rounds = 30, train_from = 3, device = 0, deterministic = 0, max_len = 0;
     uint64_t seed = 1;
     uint32_t master_rows = 0, workers = 0;
     int autotune = 1;
@@ -99,14 +108,18 @@ Options parse(int argc, char **argv) {
         else if (a == "-iter") o.iter = i32();
         else if (a == "-min-count") o.min_count = i32();
         else if (a == "-emb_output" || a == "-eoutput") o.emb_output = val();
-        else if (a == "-threads" || a == "-debug" || a == "-reuse-neg" || a == "-train" || a == "-disk" ||
-                 a == "-sync-period" || a == "-min-sync-words" || a == "-full-sync-times" || a == "-message-size")
+        else if (a == "-threads" || a == "-debug" || a == "-train" || a == "-disk" || a == "-sync-size" ||
+                 a == "-sync-period" || a == "-min-sync-words" || a == "-full-sync-times" || a == "-message-size" ||
+                 a == "-save-vocab" || a == "-read-vocab" || a == "-classes")
             val();
-        else if (a == "-hs" || a == "-cbow" || a == "-binary") {
-            if (atoi(val()) != 0) die((a + " 1 is not supported: skip-gram with negative sampling, text output").c_str());
+        else if (a == "-cbow") o.cbow = i32();
+        else if (a == "-reuse-neg") o.reuse_neg = i32();
+        else if (a == "-hs" || a == "-binary") {
+            if (atoi(val()) != 0) die((a + " 1 is not supported: negative sampling, text output").c_str());
         }
         else if (a == "-mode") o.mode = val();
         else if (a == "-lr") o.lr = val();
+        else if (a == "-lr-start") o.lr_start = static_cast<float>(atof(val()));
         else if (a == "-rounds") o.rounds = i32();
         else if (a == "-train-from") o.train_from = i32();
         else if (a == "-seed") o.seed = strtoull(val(), nullptr, 10);
@@ -123,16 +136,21 @@ Options parse(int argc, char **argv) {
     if (o.graph.empty() || o.v_num == 0 || o.walker_num == 0)
         die("usage: huge_walk -g edges.bin -v V -w W [--min_L L] [--min_R R] [--make-undirected] [-o prefix] "
             "[-size d -window k -negative n -batch-size b -sample s -alpha a -iter i -min-count c "
-            "-emb_output file] [-mode plain|plain_bf16|minibatch]");
-    if (o.mode != "plain" && o.mode != "minibatch" && o.mode != "plain_bf16")
-        die("-mode must be plain, plain_bf16 or minibatch");
+            "-emb_output file] [-cbow 0|1 -reuse-neg 0|1] [-mode plain|plain_bf16|minibatch|cbow|sg_shared]");
+    if (o.mode.empty()) o.mode = o.cbow ? "cbow" : o.reuse_neg ? "sg_shared" : "plain";
+    // word2vec.cu:1554-1555: -cbow 1 sets alpha = 0.05 unless -alpha is given (the
+    // per-round schedule then overrides it, word2vec.cu:1290).
+    if (o.mode == "cbow" && !o.alpha_set) o.alpha = 0.05f;
+    if (o.mode != "plain" && o.mode != "minibatch" && o.mode != "plain_bf16" && o.mode != "cbow" &&
+        o.mode != "sg_shared")
+        die("-mode must be plain, plain_bf16, minibatch, cbow or sg_shared");
     if (o.rounds < 1 || o.rounds > 30) die("-rounds must be 1..30 (walk.hpp:740 stops after round 30)");
     return o;
 }
 
 std::unique_ptr<dg_host::LR> make_lr(const Options &o) {
-    // word2vec.cu:1279 hard-codes ExponentialDecayLR(0.025, 0.1); -alpha sets its start here.
-    const float a0 = o.alpha_set ? o.alpha : 0.025f;
+    // word2vec.cu:1279 hard-codes ExponentialDecayLR(0.025, 0.1); -lr-start moves its start.
+    const float a0 = o.lr_start;
     if (o.lr == "exp") return std::make_unique<dg_host::ExponentialDecayLR>(a0, 0.1f);
     if (o.lr == "fixed") return std::make_unique<dg_host::FixedLR>(a0);
     if (o.lr == "cosine") return std::make_unique<dg_host::CosineAnnealingLR>(a0, a0 * 1e-4f, o.rounds);
@@ -173,7 +191,11 @@ int main(int argc, char **argv) {
     sp.alpha = o.alpha;
     sp.iter = o.iter;
     sp.min_count = o.min_count;
-    sp.mode = o.mode == "plain" ? DG_SGNS_PLAIN : o.mode == "plain_bf16" ? DG_SGNS_PLAIN_BF16 : DG_SGNS_MINIBATCH;
+    sp.mode = o.mode == "plain"        ? DG_SGNS_PLAIN
+              : o.mode == "plain_bf16" ? DG_SGNS_PLAIN_BF16
+              : o.mode == "cbow"       ? DG_SGNS_CBOW
+              : o.mode == "sg_shared"  ? DG_SGNS_SG_SHARED
+                                       : DG_SGNS_MINIBATCH;
     sp.deterministic = o.deterministic;
     sp.seed = o.seed;
     sp.table_size = o.table_size;

@@ -137,10 +137,18 @@ enum {
     DG_SGNS_PLAIN_BF16 = 2, /* the plain (word2vec.cu) rule on BF16 rows: FP32 arithmetic, FP32 master rows for
                                the hottest words (atomics), stochastic rounding for the rest; negative <= 8,
                                size 64, 128 or 256 */
+    DG_SGNS_CBOW = 3,       /* word2vec.cu cbow_kernel semantics (the reference's default, -cbow 1): FP32 rows,
+                               the mean of the window's context rows against the centre and per-centre
+                               negatives; negative <= 32 */
+    DG_SGNS_SG_SHARED = 4,  /* word2vec.cu __sgNegReuse semantics (-cbow 0 -reuse-neg 1): FP32 rows, one negative
+                               set per walk, the full window; negative <= 16.  Every supported size (the
+                               reference builds only 200 and 300) */
 };
 
 typedef struct {
-    int size;          /* -size: embedding dimension (multiple of 32, <= 512) */
+    int size;          /* -size: embedding dimension: 32, 64, 128, 256 or 512; the FP32 word2vec rules
+                          (DG_SGNS_PLAIN, _CBOW, _SG_SHARED, not in adjoint mode) take any size up to 512
+                          (e.g. the reference's run.sh uses 100), stored padded to the next of those */
     int window;        /* -window */
     int negative;      /* -negative */
     int batch_size;    /* -batch-size (minibatch mode; dsgl overrides it with 2*window+1, dsgl.hpp:832) */
@@ -388,23 +396,29 @@ typedef struct {
     uint64_t seed;
     uint32_t pass;             /* pass counter: one value per call, as dg_sgns_train_* count them */
     int deterministic;         /* 1: one worker, walks in order */
-    uint32_t workers;          /* concurrent workers; 0 = as many as fit.  dg_sgns_get_info reports the
-                                  staleness bound the handle path applies to the same vocabulary */
+    uint32_t workers;          /* concurrent workers (Hogwild); 0 = 128 (see below).  dg_sgns_get_info
+                                  reports the staleness bound the handle path applies to a vocabulary */
 } dg_sgns_minibatch_args;
 
 /* No counterpart in the reference.  The minibatch trainer (DG_SGNS_MINIBATCH)
- * with no allocation at all, for callers that cannot call cudaMalloc: code that
- * runs while a CUDA graph is being captured, code whose device memory belongs to
- * a framework's pool, or a latency-bound loop that cannot wait on an allocator.
+ * with no allocation at all, for callers that cannot call cudaMalloc: a host
+ * framework whose memory pool owns the device memory and forbids foreign
+ * allocations, or a latency-bound loop that cannot pay cudaMalloc / cudaFree
+ * (which can synchronise the device) or handle an allocation failure mid-run.
  * Its per-worker scratch (negative pools, cache snapshots) lives in a 16 MiB
  * device array that is part of this library and is held by every GPU that loads
  * it until the process exits; sizes whose per-worker scratch exceeds it are
- * DG_ERR_ARG, and the number of parallel workers is capped by it.  The first
- * call on a device looks up the array's device address, so make that first call
+ * DG_ERR_ARG, and the number of parallel workers is capped by it.  The first call
+ * on a device looks up the array's device address, so make that first call
  * before any stream capture.  Every call shares the array: calls whose work
- * overlaps on the GPU (other streams, other threads) race and must not be issued.
- * stream is a cudaStream_t (NULL = legacy default stream).  With info non-NULL
- * the call waits for the stream and reports the counters (train_ms = 0). */
+ * overlaps on the GPU (other streams, other threads) race and must not be
+ * issued.  stream is a cudaStream_t (NULL = legacy default stream) of the
+ * current device (another device's stream is DG_ERR_ARG).  Hogwild workers: the
+ * args' workers, capped by the array; 0 = 128, a staleness bound that holds for
+ * any vocabulary (the handle path's own bound, larger for most vocabularies, is
+ * dg_sgns_info.workers).  With info non-NULL the call waits for the stream to
+ * finish (cudaStreamSynchronize) and reports the counters (train_ms = 0); with
+ * info NULL it only enqueues work. */
 DG_API int dg_sgns_minibatch_train_noalloc(const dg_sgns_minibatch_args *args, void *stream, dg_train_info *info);
 
 #ifdef __cplusplus

@@ -120,6 +120,8 @@ uint32_t dgo_stream_acc(void *s);
 #define DGO_SUB_TAG 0x53554253u /* subsampling: counter (token index, walk, pass, tag) */
 #define DGO_WIN_TAG 0x57494E44u /* window shrink: (centre position, walk, pass, tag) */
 #define DGO_NEG_TAG 0x4E454730u /* negatives: (pair index, walk, pass, tag + j/4), word j%4 */
+#define DGO_CBOW_TAG 0x43424F57u  /* CBOW negatives: (centre position, walk, pass, tag + j/4), word j%4 */
+#define DGO_SHARE_TAG 0x53484E47u /* shared negatives of a walk: (0, walk, pass, tag + j/4), word j%4 */
 
 typedef struct {
     int d, window, negative;
@@ -156,6 +158,63 @@ int dgo_sgns_plain_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uin
                        float *syn0, float *syn1, dgo_sgns_stats *st);
 int dgo_sgns_minibatch_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
                            float *syn0, float *syn1, dgo_sgns_stats *st);
+
+/* word2vec.cu's trainers (dg_oracle_w2v.c).  Order of a dot product: the
+ * reference kernels' (a shared-memory tree for skip_gram_kernel / cbow_kernel,
+ * per-lane strided sums for __sgNegReuse) or the device kernels' warp order. */
+enum { DGO_ORDER_DEVICE = 0, DGO_ORDER_REF = 1 };
+enum { DGO_W2V_SG = 0, DGO_W2V_CBOW = 1, DGO_W2V_NEGREUSE = 2 };
+
+typedef struct {
+    int kind, d, window, negative;
+    float alpha;
+    uint32_t vocab_size;
+    uint64_t table_size;
+    const int32_t *table;
+    const float *exp_table;
+    int exact_sum; /* __sgNegReuse: 0 = reduceInWarp as the reference writes it, 1 = the warp sum */
+} dgo_w2v_cfg;
+
+/* The reference kernels on host-built sentences (token -1 = none), sentence k
+ * trained by "block" k with its LCG seeded k, sentences one after another;
+ * neg_samples[k * negative + y] = __sgNegReuse's shared negatives of sentence k. */
+int dgo_w2v_sentences(const dgo_w2v_cfg *c, const int32_t *sen, const int32_t *sent_off, uint32_t n_sent,
+                      const int32_t *neg_samples, float *syn0, float *syn1);
+/* The shared per-pair / per-centre updates (both forms). */
+void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, float *l1, const int32_t *tg, int nt,
+                     float *syn1, float *e);
+void dgo_w2v_cbow_centre(int order, int d, float alpha, const float *exp_table, const int32_t *ctx, int cw,
+                         const int32_t *tg, int nt, float *syn0, float *syn1, float *neu1, float *e);
+void dgo_w2v_reuse_pair(int order, int exact_sum, int d, float alpha, const float *exp_table, float *l1,
+                        int32_t word, const int32_t *negs, int n, float *syn1, float *e);
+/* Device forms of CBOW and of shared-negative skip-gram over walks. */
+int dgo_sgns_cbow_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                      float *syn0, float *syn1, dgo_sgns_stats *st);
+int dgo_sgns_negshare_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                          float *syn0, float *syn1, dgo_sgns_stats *st);
+
+/* dsgl's Train_SGNS_MPI compute thread in the reference's own random stream and
+ * arithmetic order (dg_oracle_sgns32.c): reproduces, bit for bit, the rows of the
+ * unmodified dsgl trainer built by `make -C oracle ref` (oracle/_ref/ref_dsgl,
+ * one compute thread).  Its minibatch step is the one dgo_sgns_minibatch_f32
+ * uses. */
+typedef struct {
+    int d, window, negative, iter;
+    float sample, alpha;        /* -sample; starting -alpha */
+    uint64_t train_words;       /* sum of the vertex counts */
+    uint32_t vocab_size;
+    uint64_t table_size;
+    const int32_t *table;       /* dsgl's unigram table (dgo_unigram_table_dsgl) */
+    const float *ran;           /* per vocabulary index: sqrtf(r) + r, r = sample * train_words / count */
+    const int32_t *v2w;         /* vertex id -> vocabulary index (dsgl's hash2v_vocab) */
+    const float *exp_table;
+    int device_order;           /* 0: the reference's GEMM order; 1: the device kernel's (split dot, fused chains) */
+} dgo_dsgl_cfg;
+
+int dgo_dsgl_ref(const dgo_dsgl_cfg *c, const int32_t *corpus, uint64_t n_tokens, float *wih, float *woh,
+                 float *alpha_out, dgo_sgns_stats *st);
+void dgo_unigram_table_dsgl(const uint32_t *cn, uint32_t vocab_size, uint64_t table_size, int threads,
+                            int32_t *table);
 
 /* FP64 SGNS loss and gradient over explicit minibatches (dg_oracle_adjoint.c). */
 int dgo_sgns_loss_grad(const double *in, const double *out, int d, uint32_t vocab_size, const uint32_t *inputs,

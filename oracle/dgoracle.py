@@ -15,6 +15,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libdgoracle.so")
 REF_WALK = os.path.join(HERE, "_ref", "ref_walk")
 REF_WALK_FMA = os.path.join(HERE, "_ref", "ref_walk_fma")
+REF_DSGL = os.path.join(HERE, "_ref", "ref_dsgl")
+REF_W2V = os.path.join(HERE, "_ref", "libref_w2v.so")
 
 EDGE_DTYPE = np.dtype([("src", "<u4"), ("dst", "<u4"), ("data", "<f4")])
 
@@ -53,8 +55,8 @@ def build_ref() -> bool:
     """Compile the reference's walk engine into oracle/_ref (needs the reference tree)."""
     if os.path.exists(REF_WALK) and os.path.exists(REF_WALK_FMA):
         return True
-    ref = os.environ.get("DG_REFERENCE_DIR", "/root/reference")
-    if not os.path.isdir(os.path.join(ref, "include")):
+    ref = os.environ.get("DG_REFERENCE_DIR", "")
+    if not ref or not os.path.isdir(os.path.join(ref, "include")):
         return False
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref}"], check=True)
     return True
@@ -98,6 +100,15 @@ def lib():
                                          C.c_void_p]
         L.dgo_sgns_minibatch_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                              C.c_void_p, C.c_void_p]
+        L.dgo_w2v_sentences.argtypes = [C.POINTER(W2vCfg), C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                        C.c_void_p, C.c_void_p]
+        L.dgo_sgns_cbow_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                        C.c_void_p]
+        L.dgo_sgns_negshare_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
+                                            C.c_void_p, C.c_void_p]
+        L.dgo_dsgl_ref.argtypes = [C.POINTER(_DsglCfg), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.c_void_p]
+        L.dgo_unigram_table_dsgl.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_void_p]
         L.dgo_sgns_loss_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_uint32, C.c_void_p, C.c_void_p,
                                          C.c_void_p, C.c_uint64, C.c_uint32, C.c_int, C.c_int, C.c_int64,
                                          C.c_void_p, C.c_void_p, C.c_void_p]
@@ -245,6 +256,105 @@ class SgnsStats(C.Structure):
     _fields_ = [("words", C.c_uint64), ("trained", C.c_uint64), ("pairs", C.c_uint64)]
 
 
+class W2vCfg(C.Structure):
+    _fields_ = [("kind", C.c_int), ("d", C.c_int), ("window", C.c_int), ("negative", C.c_int),
+                ("alpha", C.c_float), ("vocab_size", C.c_uint32), ("table_size", C.c_uint64),
+                ("table", C.c_void_p), ("exp_table", C.c_void_p), ("exact_sum", C.c_int)]
+
+
+class _DsglCfg(C.Structure):
+    _fields_ = [("d", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("iter", C.c_int),
+                ("sample", C.c_float), ("alpha", C.c_float), ("train_words", C.c_uint64),
+                ("vocab_size", C.c_uint32), ("table_size", C.c_uint64), ("table", C.c_void_p),
+                ("ran", C.c_void_p), ("v2w", C.c_void_p), ("exp_table", C.c_void_p), ("device_order", C.c_int)]
+
+
+def dsgl_vocab(counts: np.ndarray):
+    """dsgl's vocabulary (dsgl.hpp:355-378): vertices sorted by count, descending.
+    Only counts without ties give a unique order (std::sort is not stable)."""
+    counts = np.asarray(counts, dtype=np.int64)
+    order = np.argsort(-counts, kind="stable").astype(np.uint32)
+    v2w = np.empty(counts.size, np.int32)
+    v2w[order] = np.arange(counts.size, dtype=np.int32)
+    return order, v2w
+
+
+def dsgl_ref(counts: np.ndarray, corpus: np.ndarray, size: int, window: int, negative: int, sample: float,
+             alpha: float, iterations: int = 1, table_size: int = 100_000_000, device_order: bool = False):
+    """dsgl's trainer restated in its own random stream and GEMM order (dgo_dsgl_ref);
+    device_order=True evaluates each step in the device kernel's order instead.
+
+    counts: vertex_cn (int per vertex id); corpus: vertex ids with -1 after every
+    walk.  Returns (vocabulary ids, Wih, Woh, final alpha) in vocabulary order."""
+    L = lib()
+    counts = np.ascontiguousarray(counts, dtype=np.int32)
+    corpus = np.ascontiguousarray(corpus, dtype=np.int32)
+    ids, v2w = dsgl_vocab(counts)
+    vs = counts.size
+    cn_sorted = np.ascontiguousarray(counts[ids].astype(np.uint32))
+    train_words = int(counts.astype(np.int64).sum())
+    table = np.zeros(table_size, np.int32)
+    L.dgo_unigram_table_dsgl(cn_sorted.ctypes.data, vs, table_size, 2, table.ctypes.data)
+    # dsgl.hpp:933-935 reads the count at (*cn_vocab)[w] with w a vocabulary
+    # index, i.e. the count of VERTEX w, not of the word w.
+    st = np.float32(sample) * np.float32(train_words)
+    with np.errstate(divide="ignore"):
+        ratio = (st / counts.astype(np.float32)).astype(np.float32)
+    ran = (np.sqrt(ratio) + ratio).astype(np.float32)
+    exp_table = np.zeros(1001, np.float32)
+    L.dgo_exp_table(exp_table.ctypes.data)
+    wih = np.zeros(vs * size, np.float32)
+    L.dgo_init_rows(vs, size, wih.ctypes.data)
+    woh = np.zeros(vs * size, np.float32)
+    cfg = _DsglCfg(d=size, window=window, negative=negative, iter=iterations, sample=sample, alpha=alpha,
+                   train_words=train_words, vocab_size=vs, table_size=table_size, table=table.ctypes.data,
+                   ran=ran.ctypes.data, v2w=v2w.ctypes.data, exp_table=exp_table.ctypes.data,
+                   device_order=int(device_order))
+    a_out = C.c_float()
+    stats = SgnsStats()
+    rc = L.dgo_dsgl_ref(C.byref(cfg), corpus.ctypes.data, corpus.size, wih.ctypes.data, woh.ctypes.data,
+                        C.byref(a_out), C.byref(stats))
+    if rc:
+        raise RuntimeError("dgo_dsgl_ref failed")
+    return ids, wih.reshape(vs, size), woh.reshape(vs, size), a_out.value
+
+
+def write_dsgl_corpus(path: str, counts: np.ndarray, corpus: np.ndarray) -> None:
+    counts = np.ascontiguousarray(counts, dtype=np.int32)
+    corpus = np.ascontiguousarray(corpus, dtype=np.int32)
+    with open(path, "wb") as f:
+        f.write(np.uint32(counts.size).tobytes())
+        f.write(counts.tobytes())
+        f.write(np.uint64(corpus.size).tobytes())
+        f.write(corpus.tobytes())
+
+
+def read_dsgl_dump(path: str):
+    raw = open(path, "rb").read()
+    vs, d = np.frombuffer(raw[:16], np.uint64)
+    vs, d = int(vs), int(d)
+    o = 16
+    ids = np.frombuffer(raw[o:o + 4 * vs], np.uint32).copy(); o += 4 * vs
+    wih = np.frombuffer(raw[o:o + 4 * vs * d], np.float32).reshape(vs, d).copy(); o += 4 * vs * d
+    woh = np.frombuffer(raw[o:o + 4 * vs * d], np.float32).reshape(vs, d).copy(); o += 4 * vs * d
+    alpha = float(np.frombuffer(raw[o:o + 4], np.float32)[0])
+    return ids, wih, woh, alpha
+
+
+def run_ref_dsgl(workdir: str, counts: np.ndarray, corpus: np.ndarray, size: int, window: int, negative: int,
+                 sample: float, alpha: float, iterations: int = 1, sync_period: float = 5.0):
+    """Runs the reference's own dsgl (oracle/_ref/ref_dsgl, one compute thread)."""
+    cpath = os.path.join(workdir, "corpus.bin")
+    dpath = os.path.join(workdir, "dump.bin")
+    write_dsgl_corpus(cpath, counts, corpus)
+    cmd = [REF_DSGL, "--corpus", cpath, "--dump", dpath, "-size", str(size), "-window", str(window),
+           "-negative", str(negative), "-sample", repr(float(sample)), "-alpha", repr(float(alpha)),
+           "-iter", str(iterations), "-threads", "2", "-sync-period", str(sync_period), "-min-count", "0",
+           "-debug", "0", "-eoutput", os.path.join(workdir, "emb.txt")]
+    subprocess.run(cmd, check=True, capture_output=True)
+    return read_dsgl_dump(dpath)
+
+
 class Sgns:
     """FP64 SGNS checker: vocabulary, tables and both update rules."""
 
@@ -293,13 +403,21 @@ class Sgns:
                         keep_thr=self.keep_thr.ctypes.data, v2w=self.v2w.ctypes.data,
                         exp_table=self.exp_table.ctypes.data)
 
-    def train(self, offsets: np.ndarray, verts: np.ndarray, minibatch: bool = False, alpha=None):
+    def train(self, offsets: np.ndarray, verts: np.ndarray, minibatch: bool = False, alpha=None,
+              rule: str = "plain"):
+        """One pass over the walks.  rule: "plain" (skip-gram, FP64 + FP32),
+        "minibatch" (dsgl, FP64 + FP32; also selected by minibatch=True), "cbow" or
+        "negshare" (FP32 rows only, syn0_f32 / syn1_f32)."""
         offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
         verts = np.ascontiguousarray(verts, dtype=np.uint32)
         cfg = self._cfg(alpha)
         n = offsets.size - 1
         L = lib()
-        if minibatch:
+        if rule in ("cbow", "negshare"):
+            fn = L.dgo_sgns_cbow_f32 if rule == "cbow" else L.dgo_sgns_negshare_f32
+            rc = fn(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n, self.syn0_f32.ctypes.data,
+                    self.syn1_f32.ctypes.data, C.byref(self.stats_f32))
+        elif minibatch or rule == "minibatch":
             rc = L.dgo_sgns_minibatch(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n,
                                       self.syn0.ctypes.data, self.syn1.ctypes.data, C.byref(self.stats))
             rc |= L.dgo_sgns_minibatch_f32(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, n,

@@ -1,7 +1,7 @@
 """Regenerates the walk golden fixtures from the reference's own walk engine.
 
-Run in a container that has the reference tree (default /root/reference, or
-DG_REFERENCE_DIR):  python tests/golden/make_golden.py
+Run where the reference tree is (its path in DG_REFERENCE_DIR):
+  DG_REFERENCE_DIR=<reference tree> python tests/golden/make_golden.py
 
 For each small graph it writes <name>.bin (packed 12-byte edge records) and
 <name>_ref_walks.npz: the 30 per-round walk files produced by the UNMODIFIED

@@ -34,7 +34,7 @@ def test_huge_walk_files_and_embedding_bit_exact(distger_lib, oracle, tmp_path):
     out = _run(["-g", edges_path, "-v", "200", "-w", "200", "--min_L", "20", "--min_R", "5", "--make-undirected",
                 "-o", prefix, "-size", "64", "-window", "5", "-negative", "5", "-sample", "1e-3", "-alpha", "0.025",
                 "-iter", "1", "-min-count", "0", "-emb_output", emb_path, "-mode", "plain", "-deterministic", "1",
-                "-seed", str(seed), "-rounds", str(rounds), "-table-size", "100000"])
+                "-seed", str(seed), "-rounds", str(rounds), "-table-size", "100000", "-train-from", "1"])
     alphas = [float(a) for a in re.findall(r"alpha (\S+) walk", out)]
     assert len(alphas) == rounds and alphas[0] == pytest.approx(0.025)
     csr = oracle.Csr(edges, 200, undirected=True)
@@ -58,6 +58,36 @@ def _by_vertex(o, v_num):
     emb = np.zeros((v_num, o.syn0_f32.shape[1]), np.float32)
     emb[o.vocab_ids] = o.syn0_f32
     return emb
+
+
+def test_huge_walk_reference_defaults(distger_lib, oracle, tmp_path):
+    """No -mode: -cbow 1 (word2vec.cu:59) trains cbow_kernel's rule; rounds 1-2 are
+    walked but not trained and the schedule starts at 0.025 whatever -alpha says
+    (word2vec.cu:1279-1290); run.sh's dsgl flags are accepted."""
+    from distger import graphgen, lp
+    edges_path = os.path.join(GOLDEN, "tiny200.bin")
+    edges = graphgen.read_edges(edges_path)
+    emb_path = str(tmp_path / "emb.txt")
+    seed, rounds = 5, 4
+    out = _run(["-g", edges_path, "-v", "200", "-w", "200", "--min_L", "20", "--min_R", "5", "--make-undirected",
+                "-size", "64", "-iter", "1", "-threads", "10", "-window", "5", "-negative", "5", "-batch-size", "21",
+                "-min-count", "0", "-sample", "1e-3", "-alpha", "0.01", "-debug", "2", "-sync-size", "1024",
+                "-emb_output", emb_path, "-deterministic", "1", "-seed", str(seed), "-rounds", str(rounds),
+                "-table-size", "100000"])
+    assert "mode cbow" in out
+    assert out.count("(not trained)") == 2
+    alphas = [float(a) for a in re.findall(r"alpha (\S+) walk", out)]
+    assert alphas == [pytest.approx(0.025), pytest.approx(0.025 * np.exp(np.float32(-0.1)))]
+    csr = oracle.Csr(edges, 200, undirected=True)
+    want, _ = oracle.walk_rounds(csr, 200, 20, 5, rounds, seed=seed)
+    counts = (csr.out_deg + csr.in_deg).astype(np.uint32)
+    o = oracle.Sgns(counts, size=64, window=5, negative=5, sample=1e-3, alpha=0.05, min_count=0, seed=seed,
+                    table_size=100_000)
+    for r in (2, 3):
+        o.train(*want[r], alpha=np.float32(alphas[r - 2]), rule="cbow")
+    got = lp.read_embedding_text(emb_path, 200)
+    ids = np.flatnonzero(counts > 0)
+    np.testing.assert_allclose(got[ids], _by_vertex(o, 200)[ids], atol=6e-7, rtol=0)
 
 
 def test_huge_walk_rejects_bad_flags():

@@ -10,6 +10,8 @@ import subprocess
 import numpy as np
 import pytest
 
+import dgoracle
+
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 
 
@@ -99,10 +101,11 @@ def test_thresholds_match_the_acceptance_test(oracle):
             assert not (t <= (k - 1) / 2147483647.0)
 
 
-@pytest.mark.skipif(not os.path.isdir(os.environ.get("DG_REFERENCE_DIR", "/root/reference") + "/include"),
-                    reason="reference tree not present")
+@pytest.mark.skipif(not (os.path.exists(dgoracle.REF_WALK) and os.path.exists(dgoracle.REF_WALK_FMA)),
+                    reason="reference engine not built (make -C oracle ref REF=<reference tree>)")
 def test_oracle_matches_live_reference(oracle, tmp_path):
-    """Builds the reference engine from its sources and compares on a fresh graph."""
+    """Runs the reference engine (built from its sources into oracle/_ref) and
+    compares on a fresh graph."""
     from distger import graphgen
     assert oracle.build_ref()
     edges = graphgen.chung_lu(1500, 9000, 2.1, seed=3)

@@ -1,0 +1,99 @@
+"""CBOW (cbow_kernel, word2vec.cu:401-509) and shared-negative skip-gram
+(__sgNegReuse, word2vec.cu:231-303) trainers on the GPU.
+
+Deterministic mode (one warp, walks in order) is bit-exact against the FP32
+restatement's device form (oracle/dg_oracle_w2v.c: the per-centre / per-pair
+updates that its reference form shares, the latter pinned to the reference's
+own kernels by test_w2v_ref_gpu.py).  Hogwild runs (many warps) are checked
+statistically against the deterministic run: same counters, rows within the
+drift the plain trainer's Hogwild tests allow.
+"""
+import numpy as np
+import pytest
+
+from distger.sgns import SGNS
+
+pytestmark = pytest.mark.gpu
+
+
+def _walks(oracle, n_walks=120, seed=3):
+    from distger import graphgen
+    import os
+    edges = graphgen.read_edges(os.path.join(os.path.dirname(__file__), "golden", "tiny200.bin"))
+    ref = oracle.Csr(edges, 200, undirected=True)
+    rounds, _ = oracle.walk_rounds(ref, 200, 20, 5, 2, seed=seed)
+    offs = np.concatenate([rounds[0][0], rounds[1][0][1:] + rounds[0][0][-1]])
+    verts = np.concatenate([rounds[0][1], rounds[1][1]])
+    counts = (ref.out_deg + ref.in_deg).astype(np.uint32)
+    return offs[:n_walks + 1], verts[:int(offs[n_walks])], counts
+
+
+CFGS = [
+    dict(size=64, window=5, negative=5),
+    dict(size=128, window=10, negative=5),
+    dict(size=32, window=3, negative=1),
+    dict(size=128, window=2, negative=12),
+    dict(size=256, window=4, negative=3),
+]
+
+
+@pytest.mark.parametrize("rule", ["cbow", "sg_shared"])
+@pytest.mark.parametrize("cfg", CFGS, ids=lambda c: "d{size}w{window}n{negative}".format(**c))
+def test_deterministic_bit_exact(oracle, rule, cfg):
+    offs, verts, counts = _walks(oracle)
+    kw = dict(sample=1e-3, alpha=0.05 if rule == "cbow" else 0.025, min_count=0, seed=7, table_size=100_000)
+    s = SGNS(200, counts, mode=rule, deterministic=True, **cfg, **kw)
+    o = oracle.Sgns(counts, **cfg, **kw)
+    init = o.syn0_f32.copy()
+    for it in range(2):
+        info = s.train_host(offs, verts)
+        o.train(offs, verts, rule="cbow" if rule == "cbow" else "negshare")
+    rows, _ = s.embedding()
+    out = s.output_rows()
+    assert np.array_equal(rows.view(np.uint32), o.syn0_f32.view(np.uint32))
+    assert np.array_equal(out.view(np.uint32), o.syn1_f32.view(np.uint32))
+    assert info.words * 2 == o.stats_f32.words and info.pairs * 2 == o.stats_f32.pairs
+    assert not np.array_equal(rows, init)
+
+
+@pytest.mark.parametrize("rule", ["cbow", "sg_shared"])
+def test_hogwild_close_to_sequential(oracle, rule):
+    offs, verts, counts = _walks(oracle, n_walks=1000)
+    kw = dict(size=128, window=5, negative=5, sample=1e-3, alpha=0.025, min_count=0, seed=9, table_size=1_000_000)
+    seq = SGNS(200, counts, mode=rule, deterministic=True, **kw)
+    par = SGNS(200, counts, mode=rule, deterministic=False, workers=64, **kw)
+    i1 = seq.train_host(offs, verts)
+    i2 = par.train_host(offs, verts)
+    assert (i1.words, i1.trained, i1.pairs) == (i2.words, i2.trained, i2.pairs)
+    a, _ = seq.embedding()
+    b, _ = par.embedding()
+    rel = np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(a.astype(np.float64))
+    assert rel < 0.1, rel
+    assert np.isfinite(b).all()
+
+
+@pytest.mark.parametrize("rule", ["plain", "cbow", "sg_shared"])
+def test_unpadded_size_bit_exact(oracle, rule):
+    """-size 100 (the reference's run.sh): rows stored with 128 columns, the 28
+    padding columns zero; equal to the 128-column restatement started from the
+    100-column init (word2vec.cu:870-873 over rows of 100) padded with zeros."""
+    offs, verts, counts = _walks(oracle)
+    kw = dict(window=5, negative=5, sample=1e-3, alpha=0.025, min_count=0, seed=3, table_size=100_000)
+    s = SGNS(200, counts, size=100, mode=rule, deterministic=True, **kw)
+    o = oracle.Sgns(counts, size=128, **kw)
+    init100 = np.zeros(o.vocab_size * 100, np.float32)
+    oracle.lib().dgo_init_rows(o.vocab_size, 100, init100.ctypes.data)
+    o.syn0_f32[:] = 0
+    o.syn0_f32[:, :100] = init100.reshape(o.vocab_size, 100)
+    rows0, _ = s.embedding()
+    assert rows0.shape == (o.vocab_size, 100)
+    np.testing.assert_array_equal(rows0, o.syn0_f32[:, :100])
+    s.train_host(offs, verts)
+    if rule == "plain":
+        o.train(offs, verts)
+    else:
+        o.train(offs, verts, rule="cbow" if rule == "cbow" else "negshare")
+    rows, _ = s.embedding()
+    assert np.array_equal(rows.view(np.uint32), o.syn0_f32[:, :100].view(np.uint32))
+    assert np.array_equal(s.output_rows().view(np.uint32), o.syn1_f32[:, :100].view(np.uint32))
+    assert not o.syn0_f32[:, 100:].any() and not o.syn1_f32[:, 100:].any()

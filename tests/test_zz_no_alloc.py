@@ -1,14 +1,21 @@
 """The allocation-free minibatch trainer against the handle-based one.
 
 dg_sgns_minibatch_train_noalloc exists for callers that cannot allocate device
-memory (graph capture, framework-owned memory pools, latency-bound loops): the
-caller owns every buffer and the trainer's scratch lives in a fixed array inside
-the library.  Here the caller's buffers come from torch, are filled with the
-tables and initial rows of a handle-based trainer with the same parameters, and
-two calls in a row must leave the rows equal to what the handle's two
-dg_sgns_train_host calls produce (deterministic mode: identical, so the
-tolerance of the other SGNS tests, exact FP32 agreement, applies).
-This file is collected last on purpose.
+memory (a framework whose memory pool owns the device memory, a latency-bound
+loop that cannot pay cudaMalloc's device synchronisation): the caller owns every
+buffer and the trainer's scratch lives in a fixed array inside the library.
+Here the caller's buffers come from torch, are filled with the tables and
+initial rows of a handle-based trainer with the same parameters, and two calls
+in a row must leave the rows equal to what the handle's two dg_sgns_train_host
+calls produce (deterministic mode: identical, so the tolerance of the other SGNS
+tests, exact FP32 agreement, applies).  Hogwild runs (several workers racing)
+must report the handle path's counters and stay within the relative Frobenius
+distance the other Hogwild tests allow.
+
+The file sorts last so that, in a run that stops at the first failure, every
+other GPU test has run before it.  It does not depend on running last: each
+call clears the library's counters, and every test builds its own buffers and
+its own handle trainer.
 """
 import ctypes as C
 import os
@@ -82,6 +89,65 @@ def test_noalloc_minibatch_matches_handle_two_calls(distger_lib):
         exp_out = ref.output_rows()
         np.testing.assert_array_equal(_rows_from_device(in_bf, in_m, n_master), exp_in, err_msg=f"call {call}")
         np.testing.assert_array_equal(_rows_from_device(out_bf, out_m, n_master), exp_out, err_msg=f"call {call}")
+
+
+def _device_state(ref, size, n_master, dev):
+    import torch
+    t = ref.tables()
+    rows0, _ = ref.embedding()
+    vs = ref.vocab_size
+    u16 = (rows0.view(np.uint32) >> 16).astype(np.uint16)
+    st = dict(in_bf=torch.from_numpy(u16.view(np.int16).copy()).to(dev),
+              out_bf=torch.zeros((vs, size), dtype=torch.int16, device=dev),
+              in_m=torch.from_numpy(rows0[:n_master].copy()).to(dev),
+              out_m=torch.zeros((max(n_master, 1), size), dtype=torch.float32, device=dev),
+              v2w=torch.from_numpy(t["v2w"]).to(dev), keep=torch.from_numpy(t["keep_thr"].view(np.int32)).to(dev),
+              table=torch.from_numpy(t["table"]).to(dev), expt=torch.from_numpy(t["exp_table"]).to(dev))
+    torch.cuda.synchronize()
+    return st
+
+
+@pytest.mark.parametrize("size,negative,workers", [(64, 5, 8), (256, 14, 0)],
+                         ids=["8-workers", "array-bound-workers"])
+def test_noalloc_hogwild_matches_handle(distger_lib, size, negative, workers):
+    """Several workers: the same counters as the handle path with the same worker
+    count (walks are sliced per worker), rows within 5e-2 relative Frobenius norm
+    of the handle path's (both race).  size 256 with 14 negatives needs about
+    1 MB of scratch per worker, so the 16 MiB array admits 17 workers, fewer than
+    the default of 128: the handle path runs with that count."""
+    import torch
+    from distger import _lib
+    from distger._lib import check, lib
+    from distger.sgns import SGNS
+
+    (offs, verts), counts = _walks_and_counts()
+    n_master = 16
+    per_worker = (32 * negative * size * 2 + 64 * size) * 4
+    eff = min(workers or 128, (16 << 20) // per_worker)
+    kw = dict(size=size, window=5, negative=negative, sample=1e-3, alpha=0.025, min_count=0, mode="minibatch",
+              seed=5, table_size=1_000_000, master_rows=n_master)
+    ref = SGNS(200, counts, deterministic=False, workers=eff, **kw)
+    dev = torch.device("cuda:0")
+    st = _device_state(ref, size, n_master, dev)
+    want = ref.train_host(offs, verts)
+    d_off = torch.from_numpy(offs.astype(np.uint64).view(np.int64)).to(dev)
+    d_v = torch.from_numpy(verts.astype(np.uint32).view(np.int32)).to(dev)
+    torch.cuda.synchronize()
+    a = _lib.MinibatchArgs(verts=d_v.data_ptr(), offsets=d_off.data_ptr(), n_walks=offs.size - 1,
+                           v2w=st["v2w"].data_ptr(), keep_thr=st["keep"].data_ptr(), table=st["table"].data_ptr(),
+                           table_size=st["table"].numel(), exp_table=st["expt"].data_ptr(), vocab_size=ref.vocab_size,
+                           in_bf16=st["in_bf"].data_ptr(), out_bf16=st["out_bf"].data_ptr(),
+                           in_master=st["in_m"].data_ptr(), out_master=st["out_m"].data_ptr(), n_master=n_master,
+                           size=size, window=5, negative=negative, alpha=0.025, seed=5, pass_=0, deterministic=0,
+                           workers=workers)
+    got = _lib.TrainInfo()
+    check(lib().dg_sgns_minibatch_train_noalloc(C.byref(a), None, C.byref(got)))
+    assert (got.words, got.trained, got.pairs, got.rows) == (want.words, want.trained, want.pairs, want.rows)
+    for mine, theirs in ((_rows_from_device(st["in_bf"], st["in_m"], n_master), ref.embedding()[0]),
+                         (_rows_from_device(st["out_bf"], st["out_m"], n_master), ref.output_rows())):
+        assert np.isfinite(mine).all()
+        rel = np.linalg.norm(mine.astype(np.float64) - theirs) / np.linalg.norm(theirs.astype(np.float64))
+        assert rel < 5e-2, rel
 
 
 def test_noalloc_rejects_unsupported_size(distger_lib):

@@ -1316,7 +1316,7 @@ static void plain_fast_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) 
 
 template <int V, bool BF>
 static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    static_assert(kPlainShapeCount == 12, "dispatch below lists every shape");
+    static_assert(kPlainShapeCount == 13, "dispatch below lists every shape");
     switch (s->plain_shape) {
     case 0: plain_fast_launch<V, 0, BF>(s, a, ws); break;
     case 1: plain_fast_launch<V, 1, BF>(s, a, ws); break;
@@ -1330,6 +1330,7 @@ static int plain_fast_shape(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     case 9: plain_fast_launch<V, 9, BF>(s, a, ws); break;
     case 10: plain_fast_launch<V, 10, BF>(s, a, ws); break;
     case 11: plain_fast_launch<V, 11, BF>(s, a, ws); break;
+    case 12: plain_fast_launch<V, 12, BF>(s, a, ws); break;
     default: return dg::fail(DG_ERR_ARG, "plain launch shape %d out of range", s->plain_shape);
     }
     return DG_OK;
@@ -1659,9 +1660,9 @@ extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info 
         s->pass = pass0;
         return DG_OK;
     };
-    r.n_candidates = dgs::kPlainShapeCount;
+    r.n_candidates = dgs::kPlainTunedShapes;
     double best = 1e300;
-    for (int k = 0; k < dgs::kPlainShapeCount; k++) {
+    for (int k = 0; k < dgs::kPlainTunedShapes; k++) {
         s->plain_shape = k;
         double ms = 0.0;
         for (int rep = 0; rep < 2; rep++) {   // the first run warms caches

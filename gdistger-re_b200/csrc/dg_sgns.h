@@ -23,13 +23,18 @@ constexpr int kPlainThreads = 256;
 // would spill), and the pairs whose rows are staged ahead in shared memory
 // (0: sgns_plain_kernel; S >= 2: sgns_plain_pipe_kernel where it applies, else
 // sgns_plain_kernel with the same threads and cap).  Shape 0 is the default.
+// The autotuner times the first kPlainTunedShapes; the last shape, one warp per
+// block, exists so that a run with one worker is one warp of the staged kernel
+// (its exact replay test).
 struct PlainShape {
     int threads, per_sm, fit, stages;
 };
 constexpr PlainShape kPlainShapes[] = {{64, 0, 12, 2}, {256, 0, 0, 0}, {128, 0, 0, 0}, {64, 0, 0, 0},
                                        {64, 0, 12, 0}, {64, 0, 16, 0}, {256, 2, 0, 0}, {128, 4, 0, 0},
-                                       {64, 0, 0, 2},  {64, 0, 16, 2}, {64, 0, 12, 3}, {64, 0, 0, 3}};
+                                       {64, 0, 0, 2},  {64, 0, 16, 2}, {64, 0, 12, 3}, {64, 0, 0, 3},
+                                       {32, 0, 0, 2}};
 constexpr int kPlainShapeCount = (int)(sizeof(kPlainShapes) / sizeof(kPlainShapes[0]));
+constexpr int kPlainTunedShapes = 12;
 constexpr uint32_t kMasterRows = 1u << 16;        // hottest rows kept in FP32 in the minibatch form
 
 // Philox counter word 3 of each random choice (counter words 0-2: index, walk, pass).

@@ -193,6 +193,27 @@ int dgo_sgns_cbow_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint
 int dgo_sgns_negshare_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
                           float *syn0, float *syn1, dgo_sgns_stats *st);
 
+/* The staged-rows plain kernel (sgns_plain_pipe_kernel) run by one warp,
+ * modelled bit for bit (dg_oracle_pipe.c): rows of pair m copied after the
+ * updates of pairs < m - stages + 1, FP32 rows / masters updated by additions,
+ * BF16 rows (ids >= n_master when bf16) overwritten with stochastically rounded
+ * copies.  rows_in / rows_out: FP32 values (BF16 rows hold BF16-exact values). */
+typedef struct {
+    int d, window, negative, stages, bf16;
+    float alpha;
+    uint64_t seed;        /* Philox key of the trainer's draws */
+    uint32_t seed_lo;     /* low word of the seed (BF16 noise key) */
+    uint32_t pass;
+    uint32_t vocab_size, n_master;
+    uint64_t table_size;
+    const int32_t *table;
+    const uint32_t *keep_thr;
+    const int32_t *v2w;
+    const float *exp_table;
+} dgo_pipe_cfg;
+int dgo_sgns_pipe(const dgo_pipe_cfg *c, const uint64_t *offsets, const uint32_t *verts, uint32_t n_walks,
+                  float *rows_in, float *rows_out, dgo_sgns_stats *st);
+
 /* dsgl's Train_SGNS_MPI compute thread in the reference's own random stream and
  * arithmetic order (dg_oracle_sgns32.c): reproduces, bit for bit, the rows of the
  * unmodified dsgl trainer built by `make -C oracle ref` (oracle/_ref/ref_dsgl,

@@ -106,6 +106,8 @@ def lib():
                                         C.c_void_p]
         L.dgo_sgns_negshare_f32.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p,
                                             C.c_void_p, C.c_void_p]
+        L.dgo_sgns_pipe.argtypes = [C.POINTER(PipeCfg), C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
+                                    C.c_void_p]
         L.dgo_dsgl_ref.argtypes = [C.POINTER(_DsglCfg), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]
         L.dgo_unigram_table_dsgl.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_void_p]
@@ -260,6 +262,33 @@ class W2vCfg(C.Structure):
     _fields_ = [("kind", C.c_int), ("d", C.c_int), ("window", C.c_int), ("negative", C.c_int),
                 ("alpha", C.c_float), ("vocab_size", C.c_uint32), ("table_size", C.c_uint64),
                 ("table", C.c_void_p), ("exp_table", C.c_void_p), ("exact_sum", C.c_int)]
+
+
+class PipeCfg(C.Structure):
+    _fields_ = [("d", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("stages", C.c_int), ("bf16", C.c_int),
+                ("alpha", C.c_float), ("seed", C.c_uint64), ("seed_lo", C.c_uint32), ("pass_", C.c_uint32),
+                ("vocab_size", C.c_uint32), ("n_master", C.c_uint32), ("table_size", C.c_uint64),
+                ("table", C.c_void_p), ("keep_thr", C.c_void_p), ("v2w", C.c_void_p), ("exp_table", C.c_void_p)]
+
+
+def sgns_pipe(tables: dict, rows_in, rows_out, offsets, verts, size: int, window: int, negative: int, alpha: float,
+              seed: int, pass_: int, stages: int = 2, bf16: bool = False, n_master: int = 0):
+    """The one-warp staged-rows kernel modelled on the CPU (dgo_sgns_pipe); rows are
+    updated in place (C-contiguous FP32 arrays in vocabulary order)."""
+    t = tables
+    assert rows_in.flags.c_contiguous and rows_out.flags.c_contiguous
+    offsets = np.ascontiguousarray(offsets, dtype=np.uint64)
+    verts = np.ascontiguousarray(verts, dtype=np.uint32)
+    cfg = PipeCfg(d=size, window=window, negative=negative, stages=stages, bf16=int(bf16), alpha=alpha,
+                  seed=seed, seed_lo=seed & 0xFFFFFFFF, pass_=pass_, vocab_size=t["keep_thr"].size,
+                  n_master=n_master, table_size=t["table"].size, table=t["table"].ctypes.data,
+                  keep_thr=t["keep_thr"].ctypes.data, v2w=t["v2w"].ctypes.data, exp_table=t["exp_table"].ctypes.data)
+    st = SgnsStats()
+    rc = lib().dgo_sgns_pipe(C.byref(cfg), offsets.ctypes.data, verts.ctypes.data, offsets.size - 1,
+                             rows_in.ctypes.data, rows_out.ctypes.data, C.byref(st))
+    if rc:
+        raise RuntimeError(f"dgo_sgns_pipe failed ({rc})")
+    return st
 
 
 class _DsglCfg(C.Structure):

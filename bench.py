@@ -265,18 +265,11 @@ C5_REF_HOST_GB = 1.47e9 * (12 + 24 + 16 + 16) / 1e9 + 60
 
 
 def c5_reference_blocker(tmpdir=None) -> str | None:
-    """Why the reference cannot run the Twitter-shaped graph on this host, or None."""
-    need = C5_REF_HOST_GB
-    have = host_memory_gb()
-    if have < need:
-        return (f"the reference walk engine needs about {need:.0f} GB of host memory for the Twitter-shaped graph "
-                f"(records, undirected doubling, CSR and co-occurrence CSR, graph.hpp:376-472, 642-824); "
-                f"this host has {have:.0f} GB available")
-    import shutil
-    free = shutil.disk_usage(tmpdir or tempfile.gettempdir()).free / 1e9
-    if free < 40:
-        return f"the Twitter-shaped edge file (17.6 GB) does not fit the {free:.0f} GB free in the temp directory"
-    return None
+    """Why the reference's walk engine does not run the Twitter-shaped graph here."""
+    return (f"the reference walk engine must load all 1.47e9 edges first: about {C5_REF_HOST_GB:.0f} GB of host "
+            f"memory at its peak (records, undirected doubling, CSR and co-occurrence CSR, graph.hpp:376-472, "
+            f"642-824; this host has {host_memory_gb():.0f} GB available) and single-threaded passes over "
+            f"2.94e9 CSR entries, far beyond the minutes a bench run may take")
 
 
 def write_c5_edges(path: str, local: int) -> int:
@@ -801,44 +794,50 @@ def run_auc_synth(args, local):
 
 
 def run_profile_case(args, local):
-    """A small case of one kernel for ncu: the YouTube-shaped graph and trainer
-    (rows larger than L2), one walk round of --profile-walks walkers, then one
-    SGNS launch over those walks.  Prints a one-line summary."""
-    import distger
+    """A short case of one kernel for ncu: the --profile-workload graph and trainer,
+    one walk round of --profile-walks walkers (0: all V), then one SGNS launch over
+    those walks.  Prints a one-line summary.  On the YouTube-shaped graph the rows
+    exceed L2 already at 50,000 walks; the Twitter-shaped graph is for one-pass
+    metrics only (it holds tens of GB on the device)."""
+    from distger import _lib
+    from distger._lib import check, lib
     from distger.sgns import SGNS
-    edges = make_graph_edges()
-    v_num = 1_138_499
-    graph = distger.Graph(v_num, edges=edges, make_undirected=True, device=local)
-    csr = graph.csr()
-    counts = csr["out_deg"] + csr["in_deg"]
-    eng = distger.WalkEngine(device=local, seed=7)
-    eng.graph = graph
-    eng.set_init_round(10)
-    p1 = eng.run_round(v_num, 2, n_walkers=args.profile_walks)
-    p2 = eng.run_round(v_num, 3, n_walkers=args.profile_walks)
-    out = {"case": args.profile, "walks": args.profile_walks, "walk_ms": p2.info.walk_ms,
-           "draws": p2.info.draws, "footprints": p2.info.footprints}
-    if args.profile in ("sgns", "sgns_bf16", "minibatch", "adjoint"):
-        pmode = {"minibatch": "minibatch", "sgns_bf16": "plain_bf16"}.get(args.profile, "plain")
-        s = SGNS(v_num, counts, size=128, window=10, negative=5, batch_size=21, sample=1e-3, alpha=0.01, iter=1,
-                 min_count=0, mode=pmode, seed=1,
+    L = lib()
+    wl = args.profile_workload
+    w = BENCH[wl]
+    v_num = w["vertices"]
+    graph, _, _, _ = build_bench_graph(wl, local)
+    od, idg = graph.degrees()
+    counts = od + idg
+    walkers = args.profile_walks or v_num
+    wp = _lib.WalkParams(min_len=w["min_L"], init_round=w["min_R"], walker_num=v_num, max_len=w["max_len"], seed=7)
+    p1 = C.c_void_p()
+    check(L.dg_walk_run_round(graph.handle, C.byref(wp), 2, walkers, C.byref(p1)))
+    ri = _lib.RoundInfo()
+    check(L.dg_paths_get_info(p1, C.byref(ri)))
+    out = {"case": args.profile, "workload": wl, "walks": walkers, "walk_ms": ri.walk_ms, "draws": ri.draws,
+           "footprints": ri.footprints}
+    if args.profile in ("sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "sg_shared"):
+        pmode = {"minibatch": "minibatch", "sgns_bf16": "plain_bf16", "cbow": "cbow",
+                 "sg_shared": "sg_shared"}.get(args.profile, "plain")
+        s = SGNS(v_num, counts, size=w["size"], window=w["window"], negative=w["negative"], batch_size=21,
+                 sample=w["sample"], alpha=w["alpha"], iter=1, min_count=0, mode=pmode, seed=1,
                  deterministic=2 if args.profile == "adjoint" else 0, device=local)
-        if args.profile == "sgns" and not args.no_autotune:
-            # 7 shapes x 2 timed launches come first: profile with `ncu -s 14` to skip them.
-            out["autotune"] = s.autotune(p2)
-        info = s.train_paths(p2)
-        out.update({"train_ms": info.train_ms, "pairs": info.pairs, "words": info.words})
+        ti = _lib.TrainInfo()
+        check(L.dg_sgns_train_paths(s.handle, p1, C.c_float(0.0), C.byref(ti)))
+        out.update({"train_ms": ti.train_ms, "pairs": ti.pairs, "words": ti.words})
         s.close()
-    p1.close()
-    p2.close()
+    L.dg_paths_free(p1)
+    graph.close()
     print(json.dumps(out))
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["walk", "sgns", "sgns_bf16", "minibatch", "adjoint"], default=None,
-                    help="run one small launch of a kernel for ncu and exit")
-    ap.add_argument("--profile-walks", type=int, default=50_000)
+    ap.add_argument("--profile", choices=["walk", "sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "sg_shared"],
+                    default=None, help="run one launch of a kernel for ncu and exit")
+    ap.add_argument("--profile-walks", type=int, default=50_000, help="--profile: walkers of the round (0: all)")
+    ap.add_argument("--profile-workload", choices=sorted(BENCH), default="c2_youtube")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)

@@ -83,6 +83,52 @@ void keep_thresholds(const std::vector<uint32_t> &cn, float sample, uint64_t tra
     }
 }
 
+// CreateBinaryTree (word2vec.cu:684-740): the two smallest of the sorted counts
+// and the inner nodes made so far are merged (bit 1 for the second), then each
+// word's path is read back from the root: bit k of word a is decided by inner
+// node point[k] (0 .. n-2; the root is n-2).  Layout of InitVocabStructCUDA
+// (word2vec.cu:511-535): off[a] .. off[a+1] index word a's bits.
+bool huffman_codes(const std::vector<uint32_t> &cn, std::vector<int32_t> &off, std::vector<int32_t> &point,
+                   std::vector<int8_t> &code) {
+    const int64_t n = (int64_t)cn.size();
+    if (n < 2) return false;
+    std::vector<int64_t> count(2 * n + 1, 0), parent(2 * n + 1, 0);
+    std::vector<int8_t> binary(2 * n + 1, 0);
+    for (int64_t a = 0; a < n; a++) count[a] = cn[a];
+    for (int64_t a = n; a < 2 * n; a++) count[a] = (int64_t)1e15;
+    int64_t p1 = n - 1, p2 = n;
+    for (int64_t a = 0; a + 1 < n; a++) {
+        int64_t m[2];
+        for (int k = 0; k < 2; k++) m[k] = (p1 >= 0 && count[p1] < count[p2]) ? p1-- : p2++;
+        count[n + a] = count[m[0]] + count[m[1]];
+        parent[m[0]] = parent[m[1]] = n + a;
+        binary[m[1]] = 1;
+    }
+    off.assign(n + 1, 0);
+    point.clear();
+    code.clear();
+    int64_t path[41];
+    int8_t bits[41];
+    for (int64_t a = 0; a < n; a++) {
+        int len = 0;
+        int64_t b = a;
+        for (;;) {
+            if (len == 40) return false;   // beyond the reference's MAX_CODE_LENGTH
+            bits[len] = binary[b];
+            path[len] = b;
+            len++;
+            b = parent[b];
+            if (b == 2 * n - 2) break;
+        }
+        for (int k = 0; k < len; k++) {
+            code.push_back(bits[len - 1 - k]);
+            point.push_back(k == 0 ? (int32_t)(n - 2) : (int32_t)(path[len - k] - n));
+        }
+        off[a + 1] = (int32_t)point.size();
+    }
+    return true;
+}
+
 // expTable (word2vec.cu:1569-1573).
 void exp_table(std::vector<float> &t) {
     t.assign(kExpTableSize + 1, 0.0f);
@@ -1354,6 +1400,7 @@ static int launch_plain_bf16(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 
 int launch_plain(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     if (s->p.mode == DG_SGNS_PLAIN_BF16) return launch_plain_bf16(s, a, ws);
+    if (a.hs) return launch_plain_hs(s, a, ws);
     const int vec = s->p.size / 32;
     int blocks = 1, threads = 32;
     auto occ = [&](auto kern) {
@@ -1445,6 +1492,7 @@ dg_sgns::~dg_sgns() {
         dg::DeviceGuard guard(device);
         cudaStreamSynchronize(stream);
         v2w.release(); keep_thr.release(); table.release(); exp_table.release();
+        hs_off.release(); hs_point.release(); hs_code.release();
         syn0.release(); syn1.release(); in_bf.release(); out_bf.release(); in_master.release(); out_master.release();
         scratch.release(); queue.release(); stats.release(); adj_in.release(); adj_out.release(); adj_flag.release();
         adj_offs.release(); adj_pin.release(); adj_pout.release(); adj_neg.release(); adj_step.release();
@@ -1477,6 +1525,9 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CHECK(p->deterministic != 2 || p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH ||
                  p->mode == DG_SGNS_PLAIN_BF16,
              DG_ERR_ARG, "adjoint mode trains the skip-gram rules only");
+    DG_CHECK(!p->hs || (p->deterministic != 2 && (p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_CBOW ||
+                                                  p->mode == DG_SGNS_SG_SHARED)),
+             DG_ERR_ARG, "hierarchical softmax (hs) is available in the FP32 word2vec rules, not in adjoint mode");
     DG_CHECK(p->mode != DG_SGNS_PLAIN_BF16 || ((p->size == 64 || p->size == 128 || p->size == 256) && p->negative <= 8),
              DG_ERR_ARG, "the BF16 plain trainer supports size 64, 128 or 256 and negative <= 8");
     DG_CHECK(p->iter >= 1, DG_ERR_ARG, "iter must be >= 1");
@@ -1509,6 +1560,13 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     if (p->deterministic == 2)
         s->adj_step_batches = dgs::adjoint_step_bound(
             s->vocab_cn, thr, p->batch_size > 0 ? p->batch_size : 2 * p->window + 1, p->negative);
+    std::vector<int32_t> hs_off, hs_point;
+    std::vector<int8_t> hs_code;
+    const bool use_hs = p->hs && p->mode != DG_SGNS_SG_SHARED;   // __sgNegReuse has no HS branch
+    if (use_hs)
+        DG_CHECK(huffman_codes(s->vocab_cn, hs_off, hs_point, hs_code), DG_ERR_ARG,
+                 "hierarchical softmax needs at least 2 words and codes of at most 40 bits (word2vec.cu:33)");
+    s->p.hs = use_hs ? 1 : 0;
     std::vector<int32_t> table;
     unigram_table(s->vocab_cn, s->p.table_size, table);
     std::vector<float> et;
@@ -1526,6 +1584,17 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CUDA(cudaMemcpyAsync(s->keep_thr.p, thr.data(), thr.size() * 4, cudaMemcpyHostToDevice, s->stream));
     DG_CUDA(cudaMemcpyAsync(s->table.p, table.data(), table.size() * 4, cudaMemcpyHostToDevice, s->stream));
     DG_CUDA(cudaMemcpyAsync(s->exp_table.p, et.data(), et.size() * 4, cudaMemcpyHostToDevice, s->stream));
+    if (use_hs) {
+        DG_CUDA(s->hs_off.alloc(hs_off.size()));
+        DG_CUDA(s->hs_point.alloc(hs_point.size()));
+        DG_CUDA(s->hs_code.alloc(hs_code.size()));
+        DG_CUDA(cudaMemcpyAsync(s->hs_off.p, hs_off.data(), hs_off.size() * 4, cudaMemcpyHostToDevice, s->stream));
+        DG_CUDA(cudaMemcpyAsync(s->hs_point.p, hs_point.data(), hs_point.size() * 4, cudaMemcpyHostToDevice,
+                                s->stream));
+        DG_CUDA(cudaMemcpyAsync(s->hs_code.p, hs_code.data(), hs_code.size(), cudaMemcpyHostToDevice, s->stream));
+        // The host vectors are freed on return: the copies must have read them.
+        DG_CUDA(cudaStreamSynchronize(s->stream));
+    }
     const uint64_t n = (uint64_t)s->vocab_size * s->p.size;
     const int blocks = dg::sm_count(device) * 8;
     if (p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED) {
@@ -1582,6 +1651,10 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
     a.seed_hi = (uint32_t)(s->p.seed >> 32);
     a.deterministic = s->p.deterministic;
     a.train_words = s->train_words;
+    a.hs = s->p.hs;
+    a.hs_off = s->hs_off.p;
+    a.hs_point = s->hs_point.p;
+    a.hs_code = s->hs_code.p;
     DG_CUDA(cudaMemsetAsync(s->stats.p, 0, 4 * sizeof(unsigned long long), s->stream));
     dg::EventTimer t;
     t.start(s->stream);
@@ -1629,7 +1702,7 @@ extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info 
     DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_autotune: NULL argument");
     dg_tune_info r{};
     if (s->p.mode == DG_SGNS_MINIBATCH || s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_SG_SHARED ||
-        s->p.deterministic || s->p.negative > dgs::kFastNeg) {
+        s->p.deterministic || s->p.negative > dgs::kFastNeg || s->p.hs) {
         r.n_candidates = 1;
         r.chosen = 0;
         if (info) *info = r;

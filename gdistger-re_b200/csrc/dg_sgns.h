@@ -84,6 +84,9 @@ struct SgnsArgs {
     float alpha;
     uint32_t pass, seed_lo, seed_hi;
     int deterministic;
+    int hs;                             // hierarchical softmax: Huffman paths below
+    const int32_t *hs_off, *hs_point;   // [vocab + 1] code-length prefix; inner node per bit
+    const int8_t *hs_code;              // bit per path entry
 };
 
 // Warp sums of M per-lane partials v[0..M) (M a power of two <= 32) for the cost
@@ -120,6 +123,12 @@ bool bf_staging_safe(const std::vector<uint32_t> &cn, uint32_t n_master, int neg
 int launch_minibatch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 // cbow_kernel and __sgNegReuse semantics (dg_sgns_w2v.cu).
 int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+int launch_plain_hs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
+// word2vec's Huffman coding (CreateBinaryTree, word2vec.cu:684-740) of counts in
+// vocabulary order, laid out as off[n + 1] / point / code.  false if a code
+// would exceed the reference's 40 bits.
+bool huffman_codes(const std::vector<uint32_t> &cn, std::vector<int32_t> &off, std::vector<int32_t> &point,
+                   std::vector<int8_t> &code);
 int launch_negshare(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws);
 constexpr int kCbowMaxNeg = 32;   // one negative per lane
 constexpr int kShareMaxNeg = 16;  // shared negatives held in shared memory per warp
@@ -191,6 +200,8 @@ struct dg_sgns {
     cudaGraphExec_t adj_exec = nullptr;                 // adjoint mode: kAdjGraphSteps steps, captured once
     const void *adj_exec_key[3] = {nullptr, nullptr, nullptr};  // buffers the captured graph points at
     uint64_t adj_exec_k = 0;
+    dg::DevArray<int32_t> hs_off, hs_point;   // hierarchical softmax: Huffman paths (dgs::huffman_codes)
+    dg::DevArray<int8_t> hs_code;
     dg::DevArray<uint32_t> queue;
     dg::DevArray<unsigned long long> stats;
     dg::DevArray<uint64_t> host_off;     // dg_sgns_train_host: device copies of the caller's walks,

@@ -45,6 +45,37 @@ __device__ __forceinline__ void zero_row(RowVec<VEC> &r) {
     for (int i = 0; i < VEC; i++) r.v[i] = 0.f;
 }
 
+// Hierarchical softmax over the Huffman path of `word` (word2vec.cu:334-356,
+// 436-455): per inner node, f = x . syn1[node]; nodes with |f| >= MAX_EXP are
+// skipped, else g = (1 - code - sigmoid(f)) alpha, e += g syn1[node] (fused),
+// syn1[node] += rounded g x.  Inner nodes index the same output table as the
+// words, so every node row is read before and written after its own update.
+template <int VEC>
+__device__ __forceinline__ void hs_path(const SgnsArgs &a, int32_t word, const RowVec<VEC> &x, RowVec<VEC> &e,
+                                        uint32_t lane) {
+    const int d = 32 * VEC;
+    const int32_t k0 = a.hs_off[word], k1 = a.hs_off[word + 1];
+    for (int32_t k = k0; k < k1; k++) {
+        float *rp = a.syn1 + (size_t)a.hs_point[k] * d + lane * VEC;
+        RowVec<VEC> row;
+        load_row<VEC>(rp, row);
+        const float f = warp_dot<VEC>(x, row);
+        if (f <= -kMaxExp || f >= kMaxExp) continue;
+        const float g =
+            ((float)(1 - a.hs_code[k]) - __ldg(a.exp_table + (int)((f + kMaxExp) * (kExpTableSize / kMaxExp / 2)))) *
+            a.alpha;
+        RowVec<VEC> upd;
+#pragma unroll
+        for (int i = 0; i < VEC; i++) {
+            e.v[i] = fmaf(g, row.v[i], e.v[i]);
+            upd.v[i] = __fmul_rn(g, x.v[i]);
+            row.v[i] += upd.v[i];
+        }
+        if (a.deterministic) store_row<VEC>(rp, row);
+        else add_row<VEC>(rp, upd);
+    }
+}
+
 // ------------------------------------------------------------------ CBOW
 
 // G: target rows fetched together (their loads overlap); later groups are
@@ -101,6 +132,7 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_cbow_kernel(SgnsArgs a, Walk
             const int nt = 1 + (a.vocab_size > 1 ? a.negative : 0);
             RowVec<VEC> e;
             zero_row(e);
+            if (a.hs) hs_path<VEC>(a, word, neu1, e, lane);
             for (int g0 = 0; g0 < nt; g0 += G) {
                 int32_t t[G];
                 RowVec<VEC> row[G];
@@ -296,6 +328,80 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, 
     }
 }
 
+// ------------------------------------------- skip-gram with hierarchical softmax
+
+// skip_gram_kernel with -hs 1 (word2vec.cu:330-397): per (context, centre) pair
+// the centre's Huffman path, then the positive and the negatives (the plain
+// kernels' draws), every target row read before and written after its own update,
+// then the context row.  No row is kept in registers across pairs: an inner node
+// can be the row of the centre word itself.
+template <int VEC>
+__global__ void __launch_bounds__(kW2vThreads) sgns_plain_hs_kernel(SgnsArgs a, WalkSet ws) {
+    __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
+    const uint32_t lane = threadIdx.x & 31;
+    int32_t *sen = sen_all[threadIdx.x >> 5];
+    const int d = 32 * VEC;
+    const uint32_t w = (uint32_t)a.window;
+    const int neg = a.vocab_size > 1 ? a.negative : 0;
+    unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
+    for (;;) {
+        uint32_t walk = 0;
+        if (lane == 0) walk = atomicAdd(a.queue, 1u);
+        walk = __shfl_sync(0xffffffffu, walk, 0);
+        if (walk >= ws.n_walks) break;
+        const uint32_t wid = ws.ids ? ws.ids[walk] : walk + ws.id_base;
+        uint32_t words;
+        const uint32_t n = warp_sentence(ws, walk, a, sen, words);
+        n_words += words;
+        n_trained += n;
+        for (uint32_t p = 0; p < n; p++) {
+            const int32_t word = sen[p];
+            const uint32_t b = philox(p, wid, a.pass, kWinTag, a.seed_lo, a.seed_hi).x % w;
+            const uint32_t lo = max(b, w > p ? w - p : 0u), hi = min(2 * w + 1 - b, n + w - p);
+            for (uint32_t s = lo; s < hi; s++) {
+                if (s == w) continue;
+                n_pairs++;
+                float *l1p = a.syn0 + (size_t)sen[p - w + s] * d + lane * VEC;
+                RowVec<VEC> l1, e;
+                load_row<VEC>(l1p, l1);
+                zero_row(e);
+                hs_path<VEC>(a, word, l1, e, lane);
+                for (int j = 0; j <= neg; j++) {
+                    int32_t t = word;
+                    if (j > 0) {
+                        t = tagged_negative(a, p * (2 * w + 1) + s, wid, kNegTag, j - 1);
+                        if (t == word) continue;
+                    }
+                    float *rp = a.syn1 + (size_t)t * d + lane * VEC;
+                    RowVec<VEC> row, upd;
+                    load_row<VEC>(rp, row);
+                    const float g = sg_grad(warp_dot<VEC>(l1, row), j == 0, a.exp_table, a.alpha);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) {
+                        e.v[i] = fmaf(g, row.v[i], e.v[i]);
+                        upd.v[i] = __fmul_rn(g, l1.v[i]);
+                        row.v[i] += upd.v[i];
+                    }
+                    if (a.deterministic) store_row<VEC>(rp, row);
+                    else add_row<VEC>(rp, upd);
+                }
+                if (a.deterministic) {
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) l1.v[i] = l1.v[i] + e.v[i];
+                    store_row<VEC>(l1p, l1);
+                } else {
+                    add_row<VEC>(l1p, e);
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        atomicAdd(&a.stats[0], n_words);
+        atomicAdd(&a.stats[1], n_trained);
+        atomicAdd(&a.stats[2], n_pairs);
+    }
+}
+
 // --------------------------------------------------------------- launchers
 
 template <typename K>
@@ -351,6 +457,28 @@ int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
         case 4: return cbow_launch<4>(s, a, ws);
         case 8: return cbow_launch<8>(s, a, ws);
         case 16: return cbow_launch<16>(s, a, ws);
+        default: return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
+    }
+}
+
+template <int V>
+static int plain_hs_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    auto kern = sgns_plain_hs_kernel<V>;
+    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
+    kern<<<blocks, threads, 0, s->stream>>>(a, ws);
+    dg::note_launch();
+    DG_CUDA(cudaGetLastError());
+    return DG_OK;
+}
+
+int launch_plain_hs(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    switch (s->p.size / 32) {
+        case 1: return plain_hs_launch<1>(s, a, ws);
+        case 2: return plain_hs_launch<2>(s, a, ws);
+        case 4: return plain_hs_launch<4>(s, a, ws);
+        case 8: return plain_hs_launch<8>(s, a, ws);
+        case 16: return plain_hs_launch<16>(s, a, ws);
         default: return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
     }
 }

@@ -44,7 +44,8 @@ class SgnsParams(C.Structure):
     _fields_ = [("size", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("batch_size", C.c_int),
                 ("sample", C.c_float), ("alpha", C.c_float), ("iter", C.c_int), ("min_count", C.c_int),
                 ("mode", C.c_int), ("deterministic", C.c_int), ("seed", C.c_uint64),
-                ("table_size", C.c_uint64), ("master_rows", C.c_uint32), ("workers", C.c_uint32)]
+                ("table_size", C.c_uint64), ("master_rows", C.c_uint32), ("workers", C.c_uint32),
+                ("hs", C.c_int)]
 
 
 class TrainInfo(C.Structure):

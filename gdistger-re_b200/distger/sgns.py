@@ -26,14 +26,14 @@ class SGNS:
     def __init__(self, v_num: int, vertex_counts: np.ndarray, size: int = 128, window: int = 5, negative: int = 5,
                  batch_size: int = 11, sample: float = 1e-3, alpha: float = 0.025, iter: int = 1,
                  min_count: int = 5, mode: str = "plain", deterministic: bool = False, seed: int = 1,
-                 table_size: int = 0, master_rows: int = 0, workers: int = 0, device: int = 0):
+                 table_size: int = 0, master_rows: int = 0, workers: int = 0, device: int = 0, hs: bool = False):
         counts = np.ascontiguousarray(vertex_counts, dtype=np.uint32)
         if counts.size != v_num:
             raise ValueError("vertex_counts must have v_num entries")
         p = _lib.SgnsParams(size=size, window=window, negative=negative, batch_size=batch_size, sample=sample,
                             alpha=alpha, iter=iter, min_count=min_count, mode=MODES[mode],
                             deterministic=int(deterministic), seed=seed, table_size=table_size,
-                            master_rows=master_rows, workers=workers)
+                            master_rows=master_rows, workers=workers, hs=int(hs))
         h = C.c_void_p()
         check(lib().dg_sgns_create(C.byref(p), v_num, counts.ctypes.data, device, C.byref(h)))
         self._h = h

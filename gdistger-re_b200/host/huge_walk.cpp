@@ -23,7 +23,8 @@
 //     with -reuse-neg 1 (default, word2vec.cu:59) __sgNegReuse's shared
 //     negatives, with -reuse-neg 0 skip_gram_kernel (word2vec.cu:1073-1076, 912)
 //   -threads / -debug / -sync-size / -sync-period ...: accepted, no effect on one GPU
-//   -hs, -binary: only 0 is supported (negative sampling, text output)
+//   -hs 0|1 (default 0, word2vec.cu:66): hierarchical softmax before negative sampling
+//   -binary: only 0 is supported (text output)
 // Added for the GPU build:
 //   -mode plain|plain_bf16|minibatch|cbow|sg_shared   trainer form, overriding -cbow /
 //                           -reuse-neg (plain = skip_gram_kernel on FP32 rows;
@@ -60,7 +61,7 @@ struct Options {
     int size = 100, window = 5, negative = 5, batch_size = 11, iter = 5, min_count = 5;
     float sample = 1e-3f, alpha = 0.025f, lr_start = 0.025f;
     bool alpha_set = false;
-    int cbow = 1, reuse_neg = 1;  // word2vec.cu:59
+    int cbow = 1, reuse_neg = 1, hs = 0;  // word2vec.cu:59, 66
     int rounds = 30, train_from = 3, device = 0, deterministic = 0, max_len = 0;
     uint64_t seed = 1;
     uint32_t master_rows = 0, workers = 0;
@@ -114,8 +115,9 @@ Options parse(int argc, char **argv) {
             val();
         else if (a == "-cbow") o.cbow = i32();
         else if (a == "-reuse-neg") o.reuse_neg = i32();
-        else if (a == "-hs" || a == "-binary") {
-            if (atoi(val()) != 0) die((a + " 1 is not supported: negative sampling, text output").c_str());
+        else if (a == "-hs") o.hs = i32();
+        else if (a == "-binary") {
+            if (atoi(val()) != 0) die("-binary 1 is not supported: the embedding is written as text");
         }
         else if (a == "-mode") o.mode = val();
         else if (a == "-lr") o.lr = val();
@@ -201,6 +203,7 @@ int main(int argc, char **argv) {
     sp.table_size = o.table_size;
     sp.master_rows = o.master_rows;
     sp.workers = o.workers;
+    sp.hs = o.hs;
     dg_sgns *s = nullptr;
     check(dg_sgns_create(&sp, o.v_num, counts.data(), o.device, &s), "dg_sgns_create");
     dg_sgns_info si{};

@@ -169,6 +169,12 @@ typedef struct {
     uint32_t workers;     /* concurrent trainer workers (warps in plain mode, CTAs in minibatch mode);
                              0 = automatic; capped at what the GPU holds resident.  Adjoint mode:
                              minibatches per gradient step (0 = automatic bound) */
+    int hs;               /* -hs 1: hierarchical softmax over word2vec's Huffman coding of the vocabulary
+                             (CreateBinaryTree, word2vec.cu:684-740) before the negative-sampling
+                             targets, in DG_SGNS_PLAIN and DG_SGNS_CBOW (word2vec.cu:334-356, 436-455;
+                             inner nodes share the output rows with the words, as in the reference);
+                             no effect on DG_SGNS_SG_SHARED, as __sgNegReuse has no HS branch;
+                             not available in the BF16, minibatch or adjoint forms */
 } dg_sgns_params;
 
 /* Vocabulary from per-vertex counts (word2vec.cu:791-809 uses in+out degree,

@@ -134,6 +134,10 @@ typedef struct {
     const uint32_t *keep_thr;
     const int32_t *v2w;
     const float *exp_table;
+    int hs;                 /* hierarchical softmax (word2vec -hs 1) with the codes below */
+    const int32_t *hs_off;  /* [vocab_size + 1] prefix of the code lengths (dgo_huffman) */
+    const int32_t *hs_point;
+    const int8_t *hs_code;
 } dgo_sgns_cfg;
 
 typedef struct {
@@ -173,6 +177,9 @@ typedef struct {
     const int32_t *table;
     const float *exp_table;
     int exact_sum; /* __sgNegReuse: 0 = reduceInWarp as the reference writes it, 1 = the warp sum */
+    int hs;        /* hierarchical softmax with the codes below (skip_gram_kernel, cbow_kernel) */
+    const int32_t *hs_off, *hs_point;
+    const int8_t *hs_code;
 } dgo_w2v_cfg;
 
 /* The reference kernels on host-built sentences (token -1 = none), sentence k
@@ -180,11 +187,16 @@ typedef struct {
  * neg_samples[k * negative + y] = __sgNegReuse's shared negatives of sentence k. */
 int dgo_w2v_sentences(const dgo_w2v_cfg *c, const int32_t *sen, const int32_t *sent_off, uint32_t n_sent,
                       const int32_t *neg_samples, float *syn0, float *syn1);
-/* The shared per-pair / per-centre updates (both forms). */
-void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, float *l1, const int32_t *tg, int nt,
-                     float *syn1, float *e);
+/* The shared per-pair / per-centre updates (both forms); hs_point / hs_code /
+ * n_hs: the centre's hierarchical-softmax path (n_hs = 0 without -hs). */
+void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, float *l1, const int32_t *hs_point,
+                     const int8_t *hs_code, int n_hs, const int32_t *tg, int nt, float *syn1, float *e);
 void dgo_w2v_cbow_centre(int order, int d, float alpha, const float *exp_table, const int32_t *ctx, int cw,
-                         const int32_t *tg, int nt, float *syn0, float *syn1, float *neu1, float *e);
+                         const int32_t *hs_point, const int8_t *hs_code, int n_hs, const int32_t *tg, int nt,
+                         float *syn0, float *syn1, float *neu1, float *e);
+/* word2vec's Huffman coding (CreateBinaryTree, word2vec.cu:684-740) in the
+ * kernels' prefix layout; see dg_oracle_w2v.c. */
+int64_t dgo_huffman(const uint64_t *cn, uint32_t n, int32_t *off, int32_t *point, int8_t *code);
 void dgo_w2v_reuse_pair(int order, int exact_sum, int d, float alpha, const float *exp_table, float *l1,
                         int32_t word, const int32_t *negs, int n, float *syn1, float *e);
 /* Device forms of CBOW and of shared-negative skip-gram over walks. */

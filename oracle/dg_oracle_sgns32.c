@@ -112,8 +112,10 @@ int dgo_sgns_plain_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uin
                     }
                 /* The pair's arithmetic is word2vec.cu's (dgo_w2v_sg_pair); only the dot
                  * products' order is the warp's. */
-                dgo_w2v_sg_pair(DGO_ORDER_DEVICE, d, alpha, c->exp_table, syn0 + (size_t)sen[cp] * d, tg, nt, syn1,
-                                e);
+                const int n_hs = c->hs ? c->hs_off[word + 1] - c->hs_off[word] : 0;
+                dgo_w2v_sg_pair(DGO_ORDER_DEVICE, d, alpha, c->exp_table, syn0 + (size_t)sen[cp] * d,
+                                c->hs ? c->hs_point + c->hs_off[word] : NULL,
+                                c->hs ? c->hs_code + c->hs_off[word] : NULL, n_hs, tg, nt, syn1, e);
             }
         }
     }

@@ -100,13 +100,36 @@ static float dot_order(int order, const float *a, const float *b, int d) {
 
 /* ----------------------------------------------------- shared updates -- */
 
-/* One (context, centre) pair of skip_gram_kernel (word2vec.cu:358-397): for the
- * positive target tg[0] and the negatives tg[1..nt), in order, f = l1 . syn1[t],
- * g = (label - sigmoid(f)) alpha, e += g syn1[t] (fused), syn1[t] += rounded
- * g l1; then l1 += e. */
-void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, float *l1, const int32_t *tg, int nt,
-                     float *syn1, float *e) {
+/* Hierarchical softmax over the centre's Huffman path (word2vec.cu:334-356,
+ * 436-455): for each inner node point[k] with code bit code[k], f = x . syn1[node];
+ * nodes with |f| >= MAX_EXP are skipped, else g = (1 - code - sigmoid(f)) alpha,
+ * e += g syn1[node] (fused), syn1[node] += rounded g x.  The inner nodes index
+ * the same output table as the words (the reference trains both with d_syn1). */
+static void hs_path(int order, int d, float alpha, const float *exp_table, const float *x, const int32_t *point,
+                    const int8_t *code, int n_hs, float *syn1, float *e) {
+    for (int k = 0; k < n_hs; k++) {
+        float *row = syn1 + (size_t)point[k] * d;
+        const float f = dot_order(order, x, row, d);
+        if (f <= -MAX_EXP || f >= MAX_EXP) continue;
+        const float g = ((float)(1 - code[k]) - exp_table[(int)((f + MAX_EXP) * (EXP_TABLE_SIZE / MAX_EXP / 2))]) *
+                        alpha;
+        for (int i = 0; i < d; i++) {
+            e[i] = fmaf(g, row[i], e[i]);
+            const float u = g * x[i];
+            row[i] = row[i] + u;
+        }
+    }
+}
+
+/* One (context, centre) pair of skip_gram_kernel (word2vec.cu:330-397): the
+ * centre's hierarchical-softmax path first (n_hs nodes, none without -hs), then
+ * for the positive target tg[0] and the negatives tg[1..nt), in order,
+ * f = l1 . syn1[t], g = (label - sigmoid(f)) alpha, e += g syn1[t] (fused),
+ * syn1[t] += rounded g l1; then l1 += e. */
+void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, float *l1, const int32_t *hs_point,
+                     const int8_t *hs_code, int n_hs, const int32_t *tg, int nt, float *syn1, float *e) {
     for (int i = 0; i < d; i++) e[i] = 0.f;
+    hs_path(order, d, alpha, exp_table, l1, hs_point, hs_code, n_hs, syn1, e);
     for (int t = 0; t < nt; t++) {
         float *row = syn1 + (size_t)tg[t] * d;
         const float g = grad_table(dot_order(order, l1, row, d), t == 0, exp_table, alpha);
@@ -120,17 +143,19 @@ void dgo_w2v_sg_pair(int order, int d, float alpha, const float *exp_table, floa
 }
 
 /* One centre of cbow_kernel (word2vec.cu:419-505): neu1 = the mean of the
- * context rows (summed in window order, then divided by their count), targets
- * as in a skip-gram pair with neu1 in place of l1, then e added to every context
- * row in window order. */
+ * context rows (summed in window order, then divided by their count), the
+ * hierarchical-softmax path and the targets as in a skip-gram pair with neu1 in
+ * place of l1, then e added to every context row in window order. */
 void dgo_w2v_cbow_centre(int order, int d, float alpha, const float *exp_table, const int32_t *ctx, int cw,
-                         const int32_t *tg, int nt, float *syn0, float *syn1, float *neu1, float *e) {
+                         const int32_t *hs_point, const int8_t *hs_code, int n_hs, const int32_t *tg, int nt,
+                         float *syn0, float *syn1, float *neu1, float *e) {
     for (int i = 0; i < d; i++) { neu1[i] = 0.f; e[i] = 0.f; }
     for (int c = 0; c < cw; c++) {
         const float *r = syn0 + (size_t)ctx[c] * d;
         for (int i = 0; i < d; i++) neu1[i] = neu1[i] + r[i];
     }
     for (int i = 0; i < d; i++) neu1[i] = neu1[i] / (float)cw;
+    hs_path(order, d, alpha, exp_table, neu1, hs_point, hs_code, n_hs, syn1, e);
     for (int t = 0; t < nt; t++) {
         float *row = syn1 + (size_t)tg[t] * d;
         const float g = grad_table(dot_order(order, neu1, row, d), t == 0, exp_table, alpha);
@@ -178,6 +203,70 @@ void dgo_w2v_reuse_pair(int order, int exact_sum, int d, float alpha, const floa
         for (int i = 0; i < d; i++) row[i] = fmaf(g[i & 31], l1[i], row[i]);
     }
     for (int i = 0; i < d; i++) l1[i] = l1[i] + e[i];
+}
+
+/* The centre word's Huffman path (point, code, length) when the config trains
+ * hierarchical softmax, else an empty path. */
+#define HS_ARGS(c, word)                                                            \
+    ((c)->hs ? (c)->hs_point + (c)->hs_off[word] : NULL),                           \
+    ((c)->hs ? (c)->hs_code + (c)->hs_off[word] : NULL),                            \
+    ((c)->hs ? (c)->hs_off[(word) + 1] - (c)->hs_off[word] : 0)
+
+/* word2vec's Huffman coding restated (CreateBinaryTree, word2vec.cu:684-740):
+ * merge the two smallest of the sorted counts and the new inner nodes, bit 1 for
+ * the second; then each word's path from the root, laid out as the kernels read
+ * it (InitVocabStructCUDA, word2vec.cu:511-535): off[n + 1] prefix of the code
+ * lengths, point[] = the inner node (0 .. n-2) deciding each bit, code[] the
+ * bits.  cn: counts in vocabulary order (most frequent first), n >= 2; point
+ * and code hold n * 40 entries.  Returns the total length, or -1 when a code
+ * would be longer than the reference's 40 (MAX_CODE_LENGTH). */
+int64_t dgo_huffman(const uint64_t *cn, uint32_t n, int32_t *off, int32_t *point, int8_t *code) {
+    if (n < 2) return -1;
+    const uint64_t N = n;
+    long long *count = (long long *)calloc(2 * N + 1, sizeof(long long));
+    long long *binary = (long long *)calloc(2 * N + 1, sizeof(long long));
+    long long *parent = (long long *)calloc(2 * N + 1, sizeof(long long));
+    if (!count || !binary || !parent) { free(count); free(binary); free(parent); return -2; }
+    for (uint64_t a = 0; a < N; a++) count[a] = (long long)cn[a];
+    for (uint64_t a = N; a < 2 * N; a++) count[a] = (long long)1e15;
+    long long p1 = (long long)N - 1, p2 = (long long)N;
+    for (uint64_t a = 0; a + 1 < N; a++) {
+        long long m[2];
+        for (int k = 0; k < 2; k++) {
+            if (p1 >= 0 && count[p1] < count[p2]) m[k] = p1--;
+            else m[k] = p2++;
+        }
+        count[N + a] = count[m[0]] + count[m[1]];
+        parent[m[0]] = (long long)(N + a);
+        parent[m[1]] = (long long)(N + a);
+        binary[m[1]] = 1;
+    }
+    int64_t total = 0;
+    long long path[64];
+    int8_t bits[64];
+    off[0] = 0;
+    for (uint64_t a = 0; a < N; a++) {
+        int len = 0;
+        long long b = (long long)a;
+        while (len < 64) {
+            bits[len] = (int8_t)binary[b];
+            path[len] = b;
+            len++;
+            b = parent[b];
+            if (b == (long long)(2 * N - 2)) break;
+        }
+        if (len > 40) { total = -1; break; }
+        /* Bit k (from the root) is decided by point[k]: the root n - 2 first, then
+         * the inner nodes on the way down. */
+        for (int k = 0; k < len; k++) {
+            code[total + k] = bits[len - 1 - k];
+            point[total + k] = k == 0 ? (int32_t)(N - 2) : (int32_t)(path[len - k] - (long long)N);
+        }
+        total += len;
+        off[a + 1] = (int32_t)total;
+    }
+    free(count); free(binary); free(parent);
+    return total;
 }
 
 /* ------------------------------------------------------ reference form -- */
@@ -228,8 +317,8 @@ int dgo_w2v_sentences(const dgo_w2v_cfg *c, const int32_t *sen, const int32_t *s
                         const int32_t t = lcg_negative(c, &nr);
                         if (t != word) tg[nt++] = t;
                     }
-                    dgo_w2v_sg_pair(DGO_ORDER_REF, d, c->alpha, c->exp_table, syn0 + (size_t)sen[cp] * d, tg, nt,
-                                    syn1, e);
+                    dgo_w2v_sg_pair(DGO_ORDER_REF, d, c->alpha, c->exp_table, syn0 + (size_t)sen[cp] * d,
+                                    HS_ARGS(c, word), tg, nt, syn1, e);
                 }
             } else {
                 int cw = 0;
@@ -246,7 +335,8 @@ int dgo_w2v_sentences(const dgo_w2v_cfg *c, const int32_t *sen, const int32_t *s
                     const int32_t t = lcg_negative(c, &nr);
                     if (t != word) tg[nt++] = t;
                 }
-                dgo_w2v_cbow_centre(DGO_ORDER_REF, d, c->alpha, c->exp_table, ctx, cw, tg, nt, syn0, syn1, neu1, e);
+                dgo_w2v_cbow_centre(DGO_ORDER_REF, d, c->alpha, c->exp_table, ctx, cw, HS_ARGS(c, word), tg, nt, syn0,
+                                    syn1, neu1, e);
             }
         }
     }
@@ -318,8 +408,8 @@ int dgo_sgns_cbow_f32(const dgo_sgns_cfg *c, const uint64_t *offsets, const uint
                     const int32_t t = philox_negative(c, p, w, DGO_CBOW_TAG, j);
                     if (t != word) tg[nt++] = t;
                 }
-            dgo_w2v_cbow_centre(DGO_ORDER_DEVICE, d, (float)c->alpha, c->exp_table, ctx, cw, tg, nt, syn0, syn1,
-                                neu1, e);
+            dgo_w2v_cbow_centre(DGO_ORDER_DEVICE, d, (float)c->alpha, c->exp_table, ctx, cw, HS_ARGS(c, word), tg, nt,
+                                syn0, syn1, neu1, e);
         }
     }
     free(sen); free(e); free(neu1);

@@ -108,6 +108,8 @@ def lib():
                                             C.c_void_p, C.c_void_p]
         L.dgo_sgns_pipe.argtypes = [C.POINTER(PipeCfg), C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p,
                                     C.c_void_p]
+        L.dgo_huffman.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dgo_huffman.restype = C.c_int64
         L.dgo_dsgl_ref.argtypes = [C.POINTER(_DsglCfg), C.c_void_p, C.c_uint64, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p]
         L.dgo_unigram_table_dsgl.argtypes = [C.c_void_p, C.c_uint32, C.c_uint64, C.c_int, C.c_void_p]
@@ -251,7 +253,8 @@ class _SgnsCfg(C.Structure):
     _fields_ = [("d", C.c_int), ("window", C.c_int), ("negative", C.c_int), ("alpha", C.c_double),
                 ("seed", C.c_uint64), ("pass_", C.c_uint32), ("vocab_size", C.c_uint32),
                 ("table_size", C.c_uint64), ("table", C.c_void_p), ("keep_thr", C.c_void_p),
-                ("v2w", C.c_void_p), ("exp_table", C.c_void_p)]
+                ("v2w", C.c_void_p), ("exp_table", C.c_void_p), ("hs", C.c_int), ("hs_off", C.c_void_p),
+                ("hs_point", C.c_void_p), ("hs_code", C.c_void_p)]
 
 
 class SgnsStats(C.Structure):
@@ -261,7 +264,8 @@ class SgnsStats(C.Structure):
 class W2vCfg(C.Structure):
     _fields_ = [("kind", C.c_int), ("d", C.c_int), ("window", C.c_int), ("negative", C.c_int),
                 ("alpha", C.c_float), ("vocab_size", C.c_uint32), ("table_size", C.c_uint64),
-                ("table", C.c_void_p), ("exp_table", C.c_void_p), ("exact_sum", C.c_int)]
+                ("table", C.c_void_p), ("exp_table", C.c_void_p), ("exact_sum", C.c_int), ("hs", C.c_int),
+                ("hs_off", C.c_void_p), ("hs_point", C.c_void_p), ("hs_code", C.c_void_p)]
 
 
 class PipeCfg(C.Structure):
@@ -296,6 +300,38 @@ class _DsglCfg(C.Structure):
                 ("sample", C.c_float), ("alpha", C.c_float), ("train_words", C.c_uint64),
                 ("vocab_size", C.c_uint32), ("table_size", C.c_uint64), ("table", C.c_void_p),
                 ("ran", C.c_void_p), ("v2w", C.c_void_p), ("exp_table", C.c_void_p), ("device_order", C.c_int)]
+
+
+def huffman(cn: np.ndarray):
+    """word2vec's Huffman coding restated (dgo_huffman): (off, point, code) in the
+    kernels' prefix layout for counts in vocabulary order."""
+    cn = np.ascontiguousarray(cn, dtype=np.uint64)
+    n = cn.size
+    off = np.zeros(n + 1, np.int32)
+    point = np.zeros(n * 40, np.int32)
+    code = np.zeros(n * 40, np.int8)
+    total = lib().dgo_huffman(cn.ctypes.data, n, off.ctypes.data, point.ctypes.data, code.ctypes.data)
+    if total < 0:
+        raise ValueError("Huffman code longer than 40 bits, or fewer than 2 words")
+    return off, point[:total].copy(), code[:total].copy()
+
+
+def ref_huffman(cn: np.ndarray):
+    """The reference's own CreateBinaryTree (oracle/_ref/libref_w2v.so, host code), in
+    the same prefix layout."""
+    L = C.CDLL(REF_W2V)
+    L.ref_w2v_huffman.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p, C.c_void_p]
+    cn = np.ascontiguousarray(cn, dtype=np.int64)
+    n = cn.size
+    cl = np.zeros(n, np.int32)
+    point = np.zeros(n * 40, np.int32)
+    code = np.zeros(n * 40, np.int8)
+    L.ref_w2v_huffman(cn.ctypes.data, n, cl.ctypes.data, point.ctypes.data, code.ctypes.data)
+    off = np.zeros(n + 1, np.int32)
+    off[1:] = np.cumsum(cl)
+    p = np.concatenate([point[a * 40:a * 40 + cl[a]] for a in range(n)]) if n else np.zeros(0, np.int32)
+    c = np.concatenate([code[a * 40:a * 40 + cl[a]] for a in range(n)]) if n else np.zeros(0, np.int8)
+    return off, p.astype(np.int32), c.astype(np.int8)
 
 
 def dsgl_vocab(counts: np.ndarray):
@@ -389,7 +425,7 @@ class Sgns:
 
     def __init__(self, counts: np.ndarray, size: int = 128, window: int = 10, negative: int = 5,
                  sample: float = 1e-3, alpha: float = 0.025, min_count: int = 0, seed: int = 0,
-                 table_size: int = 100_000_000, dsgl_form: bool = False):
+                 table_size: int = 100_000_000, dsgl_form: bool = False, hs: bool = False):
         L = lib()
         counts = np.ascontiguousarray(counts, dtype=np.uint32)
         v_num = counts.size
@@ -422,6 +458,9 @@ class Sgns:
         self.syn1_f32 = np.zeros((self.vocab_size, size), np.float32)
         self.stats_f32 = SgnsStats()
         self.size, self.window, self.negative, self.alpha, self.seed = size, window, negative, alpha, seed
+        self.hs = bool(hs)
+        if self.hs:
+            self.hs_off, self.hs_point, self.hs_code = huffman(self.vocab_cn)
         self.pass_ = 0
         self.stats = SgnsStats()
 
@@ -430,7 +469,10 @@ class Sgns:
                         alpha=self.alpha if alpha is None else alpha, seed=self.seed, pass_=self.pass_,
                         vocab_size=self.vocab_size, table_size=self.table.size, table=self.table.ctypes.data,
                         keep_thr=self.keep_thr.ctypes.data, v2w=self.v2w.ctypes.data,
-                        exp_table=self.exp_table.ctypes.data)
+                        exp_table=self.exp_table.ctypes.data, hs=int(self.hs),
+                        hs_off=self.hs_off.ctypes.data if self.hs else None,
+                        hs_point=self.hs_point.ctypes.data if self.hs else None,
+                        hs_code=self.hs_code.ctypes.data if self.hs else None)
 
     def train(self, offsets: np.ndarray, verts: np.ndarray, minibatch: bool = False, alpha=None,
               rule: str = "plain"):

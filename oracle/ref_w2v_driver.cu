@@ -12,6 +12,7 @@
  * with reduSize computed as TrainModelThread computes it (word2vec.cu:971-973).
  * All pointers are device pointers owned by the caller; the table must hold
  * the reference's fixed table_size (1e8, word2vec.cu:66) entries.
+ * ref_w2v_huffman() runs the reference's host-side Huffman coding.
  */
 #include "word2vec.cu"
 
@@ -45,6 +46,33 @@ int ref_w2v_launch(int kind, int d, int win, int neg, int use_hs, long long voca
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     return (int)e;
+}
+
+/* The reference's own Huffman coding (CreateBinaryTree, word2vec.cu:684-740) of
+ * n words with counts cn (in vocabulary order, most frequent first): host code,
+ * no GPU.  Writes codelen[n] and, per word, MAX_CODE_LENGTH (40) entries of
+ * point[] and code[] (only the first codelen are meaningful).  Returns 0. */
+int ref_w2v_huffman(const long long *cn, long long n, int *codelen_out, int *point_out, char *code_out) {
+    vocab_size = n;
+    vocab = (struct vocab_word *)calloc(n + 1, sizeof(struct vocab_word));
+    for (long long a = 0; a < n; a++) {
+        vocab[a].cn = cn[a];
+        vocab[a].code = (char *)calloc(MAX_CODE_LENGTH, sizeof(char));
+        vocab[a].point = (int *)calloc(MAX_CODE_LENGTH, sizeof(int));
+    }
+    CreateBinaryTree();
+    for (long long a = 0; a < n; a++) {
+        codelen_out[a] = vocab[a].codelen;
+        for (int j = 0; j < MAX_CODE_LENGTH; j++) {
+            point_out[a * MAX_CODE_LENGTH + j] = vocab[a].point[j];
+            code_out[a * MAX_CODE_LENGTH + j] = vocab[a].code[j];
+        }
+        free(vocab[a].code);
+        free(vocab[a].point);
+    }
+    free(vocab);
+    vocab = nullptr;
+    return 0;
 }
 
 /* The reference's fixed unigram-table size (word2vec.cu:66). */

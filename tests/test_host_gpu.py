@@ -91,7 +91,7 @@ def test_huge_walk_reference_defaults(distger_lib, oracle, tmp_path):
 
 
 def test_huge_walk_rejects_bad_flags():
-    r = subprocess.run([EXE, "-g", "x.bin", "-v", "10", "-w", "10", "-hs", "1"], capture_output=True, text=True)
+    r = subprocess.run([EXE, "-g", "x.bin", "-v", "10", "-w", "10", "-binary", "1"], capture_output=True, text=True)
     assert r.returncode == 2 and "not supported" in r.stderr
     r = subprocess.run([EXE, "-g", "x.bin", "-v", "10"], capture_output=True, text=True)
     assert r.returncode == 2 and "usage" in r.stderr

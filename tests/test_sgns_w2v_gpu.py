@@ -97,3 +97,26 @@ def test_unpadded_size_bit_exact(oracle, rule):
     assert np.array_equal(rows.view(np.uint32), o.syn0_f32[:, :100].view(np.uint32))
     assert np.array_equal(s.output_rows().view(np.uint32), o.syn1_f32[:, :100].view(np.uint32))
     assert not o.syn0_f32[:, 100:].any() and not o.syn1_f32[:, 100:].any()
+
+
+@pytest.mark.parametrize("rule,negative", [("plain", 5), ("plain", 0), ("cbow", 5), ("cbow", 0)])
+def test_hierarchical_softmax_bit_exact(oracle, rule, negative):
+    """-hs 1: word2vec's Huffman coding of the vocabulary (the restatement's tree is
+    pinned to the reference's CreateBinaryTree in test_oracle_huffman.py), the
+    centre's path trained before the negative-sampling targets; the inner nodes
+    share the output table with the words."""
+    offs, verts, counts = _walks(oracle)
+    kw = dict(size=64, window=5, negative=negative, sample=1e-3, alpha=0.025, min_count=0, seed=13,
+              table_size=100_000)
+    s = SGNS(200, counts, mode=rule, deterministic=True, hs=True, **kw)
+    o = oracle.Sgns(counts, hs=True, **kw)
+    for it in range(2):
+        info = s.train_host(offs, verts)
+        if rule == "plain":
+            o.train(offs, verts)
+        else:
+            o.train(offs, verts, rule="cbow")
+    rows, _ = s.embedding()
+    assert np.array_equal(rows.view(np.uint32), o.syn0_f32.view(np.uint32))
+    assert np.array_equal(s.output_rows().view(np.uint32), o.syn1_f32.view(np.uint32))
+    assert info.pairs * 2 == o.stats_f32.pairs

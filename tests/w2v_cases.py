@@ -75,7 +75,7 @@ def run_reference_kernels(c: dict, table: np.ndarray, exp_tab: np.ndarray, devic
     import dgoracle
     L = C.CDLL(dgoracle.REF_W2V)
     L.ref_w2v_launch.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_longlong, C.c_float] + \
-        [C.c_void_p] * 11 + [C.c_int]
+        [C.c_void_p] * 10 + [C.c_int]
     L.ref_w2v_launch.restype = C.c_int
     dev = torch.device("cuda", device)
     t_table = torch.from_numpy(table).to(dev)

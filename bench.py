@@ -622,7 +622,7 @@ def run_auc_ours(args, local):
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "f32" if mode == "plain" else "bf16",
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in ("plain_bf16", "minibatch") else "f32",
                           "workers": workers or res["workers"], "master_rows": args.master_rows, "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
@@ -776,7 +776,7 @@ def run_auc_synth(args, local):
         m = pairs.auc(sgns)
         t5 = time.perf_counter()
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "f32" if mode == "plain" else "bf16", "workers": res["workers"],
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in ("plain_bf16", "minibatch") else "f32", "workers": res["workers"],
                           "master_rows": args.master_rows,
                           "auc": m["auc"], "auc_cosine": m["auc_cosine"], "test_pairs": pairs.n_pos + pairs.n_neg,
                           "vertices": cfg["n"], "undirected_edges": n_edges, "rounds": len(res["rounds"]),

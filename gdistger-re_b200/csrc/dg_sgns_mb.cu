@@ -27,8 +27,11 @@
 // updated with atomics.
 //
 // The contractions are O x I x d = 7 x 40 x 128 per step for the reference
-// configuration: far below one tcgen05 tile (M >= 64) and sequential from step
-// to step, so they run on FP32 CUDA cores.
+// configuration.  They run on FP32 CUDA cores: the step is a dependent chain of
+// row loads, products and cache updates that the next step waits on, bound by
+// latency rather than arithmetic, and FP32 fused chains keep the deterministic
+// mode bit-exact against the restatement (a tensor core's accumulation order is
+// unspecified and its operands would be rounded to BF16 / TF32).
 #include "dg_sgns.h"
 
 #include <algorithm>
@@ -54,7 +57,14 @@ struct MbArgs {
 constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
 // Workers per SM the register budget is sized for (shared memory allows about
 // as many): enough residency to reach the staleness bound on large vocabularies.
-constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 6 : 3; }
+constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 5 : 3; }
+// Register cap per thread: what mb_min_blocks workers per SM leave (size 128:
+// 200, which five 64-thread workers fit and which keeps the step free of
+// spills; shared memory holds five of them too).
+constexpr int mb_max_regs(int d) {
+    return d == 128 ? 200 : (65536 / (32 * mb_warps(d) * mb_min_blocks(d)) > 255 ? 255
+                                 : 65536 / (32 * mb_warps(d) * mb_min_blocks(d)) / 8 * 8);
+}
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
     h ^= h >> 16;
@@ -170,7 +180,7 @@ constexpr uint32_t mb_smem_bytes(int d, int out, int max_in, uint32_t pool_cap) 
 
 // D: row size; OUT: output slots per step (>= negative + 2, a divisor of 32).
 template <int D, int OUT>
-__global__ void __launch_bounds__(32 * mb_warps(D), mb_min_blocks(D)) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
+__global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) sgns_mb_kernel(SgnsArgs a, WalkSet ws, MbArgs m) {
     constexpr int NW = mb_warps(D);
     constexpr int V = D / (32 * NW);
     constexpr int IPB = 32 / OUT;                   // inputs per batch of 32 corr dots

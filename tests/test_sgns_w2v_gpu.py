@@ -45,31 +45,61 @@ def test_deterministic_bit_exact(oracle, rule, cfg):
     s = SGNS(200, counts, mode=rule, deterministic=True, **cfg, **kw)
     o = oracle.Sgns(counts, **cfg, **kw)
     init = o.syn0_f32.copy()
+    words = pairs = 0
     for it in range(2):
         info = s.train_host(offs, verts)
+        words += info.words
+        pairs += info.pairs
         o.train(offs, verts, rule="cbow" if rule == "cbow" else "negshare")
     rows, _ = s.embedding()
     out = s.output_rows()
     assert np.array_equal(rows.view(np.uint32), o.syn0_f32.view(np.uint32))
     assert np.array_equal(out.view(np.uint32), o.syn1_f32.view(np.uint32))
-    assert info.words * 2 == o.stats_f32.words and info.pairs * 2 == o.stats_f32.pairs
+    assert (words, pairs) == (o.stats_f32.words, o.stats_f32.pairs)
     assert not np.array_equal(rows, init)
 
 
+@pytest.fixture(scope="module")
+def round10k():
+    import distger
+    from distger import graphgen
+    edges = graphgen.chung_lu(10_000, 100_000, 2.2, seed=0)
+    eng = distger.WalkEngine(seed=5)
+    eng.load_graph(10_000, "", make_undirected=True, edges=edges)
+    p = eng.run_round(10_000, 1)
+    od, idg = eng.graph.degrees()
+    yield p, od + idg
+    p.close()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b.astype(np.float64)))
+
+
 @pytest.mark.parametrize("rule", ["cbow", "sg_shared"])
-def test_hogwild_close_to_sequential(oracle, rule):
-    offs, verts, counts = _walks(oracle, n_walks=1000)
-    kw = dict(size=128, window=5, negative=5, sample=1e-3, alpha=0.025, min_count=0, seed=9, table_size=1_000_000)
-    seq = SGNS(200, counts, mode=rule, deterministic=True, **kw)
-    par = SGNS(200, counts, mode=rule, deterministic=False, workers=64, **kw)
-    i1 = seq.train_host(offs, verts)
-    i2 = par.train_host(offs, verts)
-    assert (i1.words, i1.trained, i1.pairs) == (i2.words, i2.trained, i2.pairs)
-    a, _ = seq.embedding()
-    b, _ = par.embedding()
-    rel = np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(a.astype(np.float64))
-    assert rel < 0.1, rel
-    assert np.isfinite(b).all()
+def test_hogwild_close_to_sequential(distger_lib, round10k, rule):
+    """Two warps racing (Hogwild) against the one-warp run on the 10,000-vertex
+    power-law graph: the same counters, and rows no further from the sequential
+    run than 3x the plain skip-gram kernel's two-warp drift plus 1e-3 (the same
+    comparison as the plain kernel's own Hogwild tests)."""
+    p, counts = round10k
+
+    def run(mode, **kw):
+        s = SGNS(10_000, counts, size=128, window=10, negative=5, sample=1e-3, alpha=0.025, min_count=0, seed=3,
+                 table_size=1_000_000, mode=mode, **kw)
+        info = s.train_paths(p)
+        out = (info, s.embedding()[0], s.output_rows())
+        s.close()
+        return out
+
+    ref_seq, ref_par = run("plain", deterministic=True), run("plain", workers=2)
+    seq, par = run(rule, deterministic=True), run(rule, workers=2)
+    assert (seq[0].words, seq[0].trained, seq[0].pairs) == (par[0].words, par[0].trained, par[0].pairs)
+    bound = 3 * max(_rel(ref_par[1], ref_seq[1]), _rel(ref_par[2], ref_seq[2])) + 1e-3
+    d = max(_rel(par[1], seq[1]), _rel(par[2], seq[2]))
+    print(f"{rule}: two-warp drift {d:.3e} (bound {bound:.3e})")
+    assert np.isfinite(par[1]).all() and np.isfinite(par[2]).all()
+    assert d <= bound
 
 
 @pytest.mark.parametrize("rule", ["plain", "cbow", "sg_shared"])
@@ -110,8 +140,9 @@ def test_hierarchical_softmax_bit_exact(oracle, rule, negative):
               table_size=100_000)
     s = SGNS(200, counts, mode=rule, deterministic=True, hs=True, **kw)
     o = oracle.Sgns(counts, hs=True, **kw)
+    pairs = 0
     for it in range(2):
-        info = s.train_host(offs, verts)
+        pairs += s.train_host(offs, verts).pairs
         if rule == "plain":
             o.train(offs, verts)
         else:
@@ -119,4 +150,4 @@ def test_hierarchical_softmax_bit_exact(oracle, rule, negative):
     rows, _ = s.embedding()
     assert np.array_equal(rows.view(np.uint32), o.syn0_f32.view(np.uint32))
     assert np.array_equal(s.output_rows().view(np.uint32), o.syn1_f32.view(np.uint32))
-    assert info.pairs * 2 == o.stats_f32.pairs
+    assert pairs == o.stats_f32.pairs

@@ -107,47 +107,77 @@ def _device_state(ref, size, n_master, dev):
     return st
 
 
+@pytest.fixture(scope="module")
+def walks10k():
+    import distger
+    from distger import graphgen
+    edges = graphgen.chung_lu(10_000, 100_000, 2.2, seed=0)
+    eng = distger.WalkEngine(seed=5)
+    eng.load_graph(10_000, "", make_undirected=True, edges=edges)
+    p = eng.run_round(10_000, 1, n_walkers=4000)
+    offs, verts = p.to_numpy()
+    od, idg = eng.graph.degrees()
+    p.close()
+    eng.graph.close()
+    return offs, verts, (od + idg).astype(np.uint32)
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a.astype(np.float64) - b) / np.linalg.norm(b.astype(np.float64)))
+
+
 @pytest.mark.parametrize("size,negative,workers", [(64, 5, 8), (256, 14, 0)],
                          ids=["8-workers", "array-bound-workers"])
-def test_noalloc_hogwild_matches_handle(distger_lib, size, negative, workers):
-    """Several workers: the same counters as the handle path with the same worker
-    count (walks are sliced per worker), rows within 5e-2 relative Frobenius norm
-    of the handle path's (both race).  size 256 with 14 negatives needs about
-    1 MB of scratch per worker, so the 16 MiB array admits 17 workers, fewer than
-    the default of 128: the handle path runs with that count."""
+def test_noalloc_hogwild_matches_handle(distger_lib, walks10k, size, negative, workers):
+    """Several workers racing on a 10,000-vertex power-law graph: the same counters
+    as the handle path with the same worker count (walks are sliced per worker),
+    and rows no further from a handle run than 3x the distance between two handle
+    runs plus 1e-3 (Hogwild runs differ from each other by their races).  size 256
+    with 14 negatives needs about 1 MB of scratch per worker, so the 16 MiB array
+    admits 17 workers, fewer than the default of 128: the handle path runs with
+    that count."""
     import torch
     from distger import _lib
     from distger._lib import check, lib
     from distger.sgns import SGNS
 
-    (offs, verts), counts = _walks_and_counts()
-    n_master = 16
+    offs, verts, counts = walks10k
+    n_master = 256
     per_worker = (32 * negative * size * 2 + 64 * size) * 4
     eff = min(workers or 128, (16 << 20) // per_worker)
     kw = dict(size=size, window=5, negative=negative, sample=1e-3, alpha=0.025, min_count=0, mode="minibatch",
               seed=5, table_size=1_000_000, master_rows=n_master)
-    ref = SGNS(200, counts, deterministic=False, workers=eff, **kw)
+    runs = []
+    for _ in range(2):
+        ref = SGNS(counts.size, counts, deterministic=False, workers=eff, **kw)
+        want = ref.train_host(offs, verts)
+        runs.append((want, ref.embedding()[0], ref.output_rows()))
+        ref.close()
+    noise = max(_rel(runs[0][1], runs[1][1]), _rel(runs[0][2], runs[1][2]))
+    ref = SGNS(counts.size, counts, deterministic=False, workers=eff, **kw)
     dev = torch.device("cuda:0")
     st = _device_state(ref, size, n_master, dev)
-    want = ref.train_host(offs, verts)
+    ref.close()
     d_off = torch.from_numpy(offs.astype(np.uint64).view(np.int64)).to(dev)
     d_v = torch.from_numpy(verts.astype(np.uint32).view(np.int32)).to(dev)
     torch.cuda.synchronize()
     a = _lib.MinibatchArgs(verts=d_v.data_ptr(), offsets=d_off.data_ptr(), n_walks=offs.size - 1,
                            v2w=st["v2w"].data_ptr(), keep_thr=st["keep"].data_ptr(), table=st["table"].data_ptr(),
-                           table_size=st["table"].numel(), exp_table=st["expt"].data_ptr(), vocab_size=ref.vocab_size,
-                           in_bf16=st["in_bf"].data_ptr(), out_bf16=st["out_bf"].data_ptr(),
-                           in_master=st["in_m"].data_ptr(), out_master=st["out_m"].data_ptr(), n_master=n_master,
-                           size=size, window=5, negative=negative, alpha=0.025, seed=5, pass_=0, deterministic=0,
-                           workers=workers)
+                           table_size=st["table"].numel(), exp_table=st["expt"].data_ptr(),
+                           vocab_size=runs[0][1].shape[0], in_bf16=st["in_bf"].data_ptr(),
+                           out_bf16=st["out_bf"].data_ptr(), in_master=st["in_m"].data_ptr(),
+                           out_master=st["out_m"].data_ptr(), n_master=n_master, size=size, window=5,
+                           negative=negative, alpha=0.025, seed=5, pass_=0, deterministic=0, workers=workers)
     got = _lib.TrainInfo()
     check(lib().dg_sgns_minibatch_train_noalloc(C.byref(a), None, C.byref(got)))
+    want = runs[0][0]
     assert (got.words, got.trained, got.pairs, got.rows) == (want.words, want.trained, want.pairs, want.rows)
-    for mine, theirs in ((_rows_from_device(st["in_bf"], st["in_m"], n_master), ref.embedding()[0]),
-                         (_rows_from_device(st["out_bf"], st["out_m"], n_master), ref.output_rows())):
-        assert np.isfinite(mine).all()
-        rel = np.linalg.norm(mine.astype(np.float64) - theirs) / np.linalg.norm(theirs.astype(np.float64))
-        assert rel < 5e-2, rel
+    mine_in = _rows_from_device(st["in_bf"], st["in_m"], n_master)
+    mine_out = _rows_from_device(st["out_bf"], st["out_m"], n_master)
+    assert np.isfinite(mine_in).all() and np.isfinite(mine_out).all()
+    d = max(_rel(mine_in, runs[0][1]), _rel(mine_out, runs[0][2]))
+    print(f"noalloc vs handle {d:.3e}, handle vs handle {noise:.3e}")
+    assert d <= 3 * noise + 1e-3
 
 
 def test_noalloc_rejects_unsupported_size(distger_lib):

@@ -7,7 +7,7 @@
 //    window's context rows, one positive and `negative` sampled targets, their
 //    gradient e added to every context row.
 //  * DG_SGNS_SG_SHARED: __sgNegReuse (word2vec.cu:231-303), the reference's
-//    skip-gram when -cbow 0 (reuseNeg = 1): one negative set per sentence, the
+//    skip-gram when -cbow 0 (reuseNeg = 1): one negative set per walk, the
 //    full window, the centre's output row as the positive, the context row
 //    updated by the pair's e.  The reference instantiates it for size 200 and
 //    300 only and exits for others (word2vec.cu:914-926); here every size the
@@ -188,26 +188,26 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_cbow_kernel(SgnsArgs a, Walk
 
 // ------------------------------------------------ shared-negative skip-gram
 
-// The walk's negative rows live in the warp's shared memory for the duration of
-// one centre (loaded at its start, written back at its end: stored in
-// deterministic mode, their change added atomically otherwise), so the up to
-// 2 * window pairs of a centre read and update them there; the centre's output
-// row (the positive) stays in registers, or is the shared copy when the centre
-// word is one of the negatives.  Shared memory per warp: the sentence, the
-// negatives, and 2 x negative rows (current and as loaded).
+// Negative rows fetched together per pair (their loads overlap).
+constexpr int kShareGroup = 4;
+
+// One negative set per walk (kept in shared memory), the full window; per pair
+// the negatives that differ from the centre, then the centre as the positive,
+// each against the unchanged context row.  Negative rows are read and written
+// at every pair, as the reference writes them (an update that a hot negative
+// row receives from another warp is seen at the next pair, so no warp holds a
+// stale copy for long); the centre's output row stays in registers for the
+// centre, as in the plain kernels.  Hogwild: vector atomics add the rounded
+// increments g*l1 (the reference adds g*l1 to the row fused, without atomics).
 template <int VEC>
 __global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, WalkSet ws) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
+    __shared__ int32_t negs_all[kW2vThreads / 32][kShareMaxNeg];
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t *sen = sen_all[warp];
+    int32_t *negs = negs_all[warp];
     const int d = 32 * VEC;
     const int neg = a.vocab_size > 1 ? a.negative : 0;
-    const size_t warp_bytes = (size_t)kMaxSentence * 4 + kShareMaxNeg * 8 + (size_t)2 * neg * d * 4;
-    unsigned char *base = smem_raw + warp * warp_bytes;
-    int32_t *sen = reinterpret_cast<int32_t *>(base);
-    int32_t *negs = reinterpret_cast<int32_t *>(base + (size_t)kMaxSentence * 4);
-    int32_t *slot = negs + kShareMaxNeg;  // slot of negative j: index of its first occurrence
-    float *cur = reinterpret_cast<float *>(base + (size_t)kMaxSentence * 4 + kShareMaxNeg * 8);
-    float *init = cur + (size_t)neg * d;
     const uint32_t w = (uint32_t)a.window;
     unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
     for (;;) {
@@ -221,33 +221,14 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, 
         n_words += words;
         n_trained += n;
         if (n < 2) continue;
-        if ((int)lane < neg) negs[lane] = tagged_negative(a, 0, wid, kShareTag, (int)lane);
         __syncwarp();
-        if ((int)lane < neg) {
-            int s = (int)lane;
-            for (int k = 0; k < (int)lane; k++)
-                if (negs[k] == negs[lane]) { s = k; break; }
-            slot[lane] = s;
-        }
+        if ((int)lane < neg) negs[lane] = tagged_negative(a, 0, wid, kShareTag, (int)lane);
         __syncwarp();
         for (uint32_t p = 0; p < n; p++) {
             const int32_t word = sen[p];
-            // This centre's rows: the distinct negatives into shared memory, the
-            // positive into registers unless it is one of them.
-            int pslot = -1;
-            for (int j = 0; j < neg; j++) {
-                if (slot[j] != j) continue;
-                if (negs[j] == word) pslot = j;
-                RowVec<VEC> r;
-                load_row<VEC>(a.syn1 + (size_t)negs[j] * d + lane * VEC, r);
-#pragma unroll
-                for (int i = 0; i < VEC; i++) cur[(size_t)j * d + lane * VEC + i] = init[(size_t)j * d + lane * VEC + i] = r.v[i];
-            }
             RowVec<VEC> pos, pos0;
-            if (pslot < 0) {
-                load_row<VEC>(a.syn1 + (size_t)word * d + lane * VEC, pos);
-                pos0 = pos;
-            }
+            load_row<VEC>(a.syn1 + (size_t)word * d + lane * VEC, pos);
+            pos0 = pos;
             const uint32_t lo = w > p ? w - p : 0u, hi = min(2 * w + 1, n + w - p);
             for (uint32_t s = lo; s < hi; s++) {
                 if (s == w) continue;
@@ -256,35 +237,43 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, 
                 RowVec<VEC> l1, e;
                 load_row<VEC>(l1p, l1);
                 zero_row(e);
-                // Negatives in order (those equal to the centre skipped), then the
-                // positive (word2vec.cu:256-297; the reference's warps y < negative,
-                // then y = negative).
-                for (int j = 0; j <= neg; j++) {
-                    float *sr = nullptr;
-                    if (j < neg) {
-                        if (negs[j] == word) continue;
-                        sr = cur + (size_t)slot[j] * d + lane * VEC;
-                    } else if (pslot >= 0) {
-                        sr = cur + (size_t)pslot * d + lane * VEC;
-                    }
-                    RowVec<VEC> r;
-                    if (sr) {
+                // Negatives in order, those equal to the centre skipped (word2vec.cu:
+                // 256-297: warps y < negative, then y = negative for the positive).
+                for (int j0 = 0; j0 < neg; j0 += kShareGroup) {
+                    int32_t t[kShareGroup];
+                    RowVec<VEC> row[kShareGroup];
 #pragma unroll
-                        for (int i = 0; i < VEC; i++) r.v[i] = sr[i];
-                    } else {
-                        r = pos;
+                    for (int k = 0; k < kShareGroup; k++) {
+                        t[k] = j0 + k < neg ? negs[j0 + k] : -1;
+                        if (t[k] == word) t[k] = -1;
+                        if (t[k] >= 0) load_row<VEC>(a.syn1 + (size_t)t[k] * d + lane * VEC, row[k]);
                     }
-                    const float g = sg_grad(warp_dot<VEC>(l1, r), j == neg, a.exp_table, a.alpha);
+#pragma unroll
+                    for (int k = 0; k < kShareGroup; k++) {
+                        if (t[k] < 0) continue;
+                        const float g = sg_grad(warp_dot<VEC>(l1, row[k]), 0, a.exp_table, a.alpha);
+                        RowVec<VEC> upd;
+#pragma unroll
+                        for (int i = 0; i < VEC; i++) {
+                            e.v[i] += __fmul_rn(g, row[k].v[i]);
+                            upd.v[i] = __fmul_rn(g, l1.v[i]);
+                            row[k].v[i] = fmaf(g, l1.v[i], row[k].v[i]);
+                        }
+                        float *rp = a.syn1 + (size_t)t[k] * d + lane * VEC;
+                        if (a.deterministic) store_row<VEC>(rp, row[k]);
+                        else add_row<VEC>(rp, upd);
+                        // A repeat of this negative later in the group sees this update.
+#pragma unroll
+                        for (int q = k + 1; q < kShareGroup; q++)
+                            if (t[q] == t[k]) row[q] = row[k];
+                    }
+                }
+                {   // the positive: the centre's output row
+                    const float g = sg_grad(warp_dot<VEC>(l1, pos), 1, a.exp_table, a.alpha);
 #pragma unroll
                     for (int i = 0; i < VEC; i++) {
-                        e.v[i] += __fmul_rn(g, r.v[i]);
-                        r.v[i] = fmaf(g, l1.v[i], r.v[i]);
-                    }
-                    if (sr) {
-#pragma unroll
-                        for (int i = 0; i < VEC; i++) sr[i] = r.v[i];
-                    } else {
-                        pos = r;
+                        e.v[i] += __fmul_rn(g, pos.v[i]);
+                        pos.v[i] = fmaf(g, l1.v[i], pos.v[i]);
                     }
                 }
                 if (a.deterministic) {
@@ -295,30 +284,14 @@ __global__ void __launch_bounds__(kW2vThreads) sgns_negshare_kernel(SgnsArgs a, 
                     add_row<VEC>(l1p, e);
                 }
             }
-            // Write the centre's rows back.
-            for (int j = 0; j < neg; j++) {
-                if (slot[j] != j) continue;
-                float *dst = a.syn1 + (size_t)negs[j] * d + lane * VEC;
-                RowVec<VEC> r;
+            float *dst = a.syn1 + (size_t)word * d + lane * VEC;
+            if (a.deterministic) {
+                store_row<VEC>(dst, pos);
+            } else {
 #pragma unroll
-                for (int i = 0; i < VEC; i++) {
-                    const float c = cur[(size_t)j * d + lane * VEC + i];
-                    r.v[i] = a.deterministic ? c : c - init[(size_t)j * d + lane * VEC + i];
-                }
-                if (a.deterministic) store_row<VEC>(dst, r);
-                else add_row<VEC>(dst, r);
+                for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
+                add_row<VEC>(dst, pos);
             }
-            if (pslot < 0) {
-                float *dst = a.syn1 + (size_t)word * d + lane * VEC;
-                if (a.deterministic) {
-                    store_row<VEC>(dst, pos);
-                } else {
-#pragma unroll
-                    for (int i = 0; i < VEC; i++) pos.v[i] -= pos0.v[i];
-                    add_row<VEC>(dst, pos);
-                }
-            }
-            __syncwarp();
         }
     }
     if (lane == 0) {
@@ -429,22 +402,12 @@ static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     return DG_OK;
 }
 
-size_t negshare_warp_bytes(int negative, int size) {
-    return (size_t)kMaxSentence * 4 + kShareMaxNeg * 8 + (size_t)2 * negative * size * 4;
-}
-
 template <int V>
 static int negshare_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     auto kern = sgns_negshare_kernel<V>;
-    const int neg = a.vocab_size > 1 ? a.negative : 0;
-    const size_t per_warp = negshare_warp_bytes(neg, s->p.size);
-    // As many warps per block (up to 8) as fit in 200 KB of shared memory.
-    const int warps = s->p.deterministic ? 1 : (int)std::max<size_t>(1, std::min<size_t>(8, (200u << 10) / per_warp));
-    const int threads = 32 * warps;
-    const size_t smem = per_warp * warps;
-    DG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, smem, s->device), threads);
-    kern<<<blocks, threads, smem, s->stream>>>(a, ws);
+    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
+    kern<<<blocks, threads, 0, s->stream>>>(a, ws);
     dg::note_launch();
     DG_CUDA(cudaGetLastError());
     return DG_OK;

@@ -196,51 +196,46 @@ def pipeline_rate(walk_steps_per_s: float, words_per_s: float) -> float:
 
 def run_reference(args, rank, world, pg):
     """The reference's own CPU implementation of the path (walk.hpp engine + dsgl,
-    oracle/_ref/ref_embed) on the host cores, on the bench workload: W + K walk
-    rounds of --ref-walkers walkers each (a prefix of the walker ids; walker w
-    starts at w % V, walk.hpp:501-509) and dsgl over the corpus of all those
-    rounds.  A step's time = its round's walk time (measured per round, without
-    the engine's dump and path assembly) + its share, by tokens, of dsgl's
-    measured time over the whole corpus; no time is extrapolated."""
+    oracle/_ref/ref_embed) on the host cores, on the bench workload.  It runs
+    W + K walk rounds of V walkers (the engine asserts that a round visits every
+    vertex, walk.hpp:723, so a round cannot be subsampled; times per round exclude
+    the engine's dump and path assembly) and dsgl on the first --ref-sgns-words
+    corpus tokens.  value = the pipeline rate of the two measured rates (each
+    footprint walked once and trained once, as in our arm); ms_per_step = the
+    measured CPU time of the K timed rounds plus the dsgl run, divided by K, so
+    ms_per_step x K is time the reference actually spent."""
     if rank != 0:
         return
     wl = args.workload_bench
     w = BENCH[wl]
     form = args.mode or w["headline"]
+    if wl == "c5_twitter":
+        print(json.dumps({"impl": "reference", "unavailable": c5_reference_blocker(args.tmpdir)}))
+        return
     from distger import graphgen
     with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
         path = os.path.join(tmp, "g.bin")
-        if wl == "c5_twitter":
-            why = c5_reference_blocker(args.tmpdir)
-            if why:
-                print(json.dumps({"impl": "reference", "unavailable": why}))
-                return
-            write_c5_edges(path, int(os.environ.get("LOCAL_RANK", "0")))
-        else:
-            graphgen.write_edges(path, make_graph_edges())
-        res = ref_baseline(path, w["vertices"], args.warmup + args.steps, 0, walkers=args.ref_walkers,
+        graphgen.write_edges(path, make_graph_edges())
+        res = ref_baseline(path, w["vertices"], args.warmup + args.steps, args.ref_sgns_words,
                            timeout=args.ref_timeout)
     if res is None or len(res["rounds"]) < args.warmup + args.steps or not res["sgns_train_s"]:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_embed missing or failed "
                           "(reference walk engine + dsgl built by make -C oracle ref)"}))
         return
-    all_fp = sum(r[1] for r in res["rounds"])
     timed = res["rounds"][args.warmup:]
-    fp = sum(r[1] for r in timed)
     walk_s = sum(r[0] for r in timed)
-    sgns_s = res["sgns_train_s"] * fp / all_fp
-    value = fp / (walk_s + sgns_s)
     walk_rate = sum(r[1] - r[2] for r in timed) / walk_s
     word_rate = res["sgns_words"] / res["sgns_train_s"]
-    sample = (f"{len(res['rounds'])} walk rounds of {args.ref_walkers} walkers on the same graph "
-              f"(walk.hpp internal_random_walk, {res['walk_threads']} threads), dsgl over their "
-              f"{res['sgns_words']} corpus tokens ({res['cores']} threads); first {args.warmup} rounds untimed")
+    value = pipeline_rate(walk_rate, word_rate)
+    sample = (f"{len(res['rounds'])} walk rounds of {w['vertices']} walkers on the same graph "
+              f"(walk.hpp internal_random_walk, {res['walk_threads']} threads; the first {args.warmup} untimed), "
+              f"dsgl on the first {res['sgns_words']} corpus tokens ({res['cores']} threads)")
     cfg = {k: v for k, v in w.items() if k not in ("headline", "source")}
-    cfg.update(workload=f"{wl}_{form}", sgns_form=form, walkers_per_round=args.ref_walkers)
+    cfg.update(workload=f"{wl}_{form}", sgns_form=form, walkers_per_round=w["vertices"])
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 0, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": 1e3 * (walk_s + sgns_s) / len(timed), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
-            "config": cfg, "walk_steps_per_s": walk_rate, "sgns_words_per_s": word_rate,
+            "warmup": args.warmup, "ms_per_step": 1e3 * (walk_s + res["sgns_train_s"]) / len(timed),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "impl": "reference", "config": cfg, "walk_steps_per_s": walk_rate, "sgns_words_per_s": word_rate,
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["cores"], "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -272,42 +267,18 @@ def c5_reference_blocker(tmpdir=None) -> str | None:
             f"2.94e9 CSR entries, far beyond the minutes a bench run may take")
 
 
-def write_c5_edges(path: str, local: int) -> int:
-    """The Twitter-shaped graph's edges (the same device generator and seed as the
-    bench graph) as the reference's 12-byte records (storage.hpp:15-37)."""
-    import numpy as np
-    from distger import graphgen
-    from distger.synth import EdgeList
-    w = BENCH["c5_twitter"]
-    e = EdgeList.chung_lu(w["vertices"], w["draws"], w["exponent"], seed=0, max_degree=float(w["max_degree"]),
-                          weighted=w["weighted"], device=local)
-    src, dst, data = e.to_numpy()
-    e.close()
-    rec = np.empty(src.size, dtype=graphgen.EDGE_DTYPE)
-    rec["src"], rec["dst"], rec["data"] = src, dst, data
-    del src, dst, data
-    graphgen.write_edges(path, rec)
-    return int(rec.size)
-
-
 def cpu_baseline(args, wl, graph, host_edges):
     """The reference's own walk engine + dsgl (oracle/_ref/ref_embed) on the box's
-    host cores, on a bounded sample of the same workload: one walk round of a
-    prefix of the walkers (walker ids 0.., starts id % V, walk.hpp:501-509) and
-    dsgl on the first --ref-sgns-words corpus tokens."""
+    host cores, on a bounded sample of the same workload: one walk round of V
+    walkers and dsgl on the first --ref-sgns-words corpus tokens."""
     from distger import graphgen
     w = BENCH[wl]
     with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
         path = os.path.join(tmp, "g.bin")
         if wl == "c5_twitter":
-            why = c5_reference_blocker(args.tmpdir)
-            if why:
-                return {"unavailable": why}
-            write_c5_edges(path, int(os.environ.get("LOCAL_RANK", "0")))
-            walkers = args.ref_walkers
-        else:
-            graphgen.write_edges(path, host_edges)
-            walkers = w["vertices"]
+            return {"unavailable": c5_reference_blocker(args.tmpdir)}
+        graphgen.write_edges(path, host_edges)
+        walkers = w["vertices"]
         res = ref_baseline(path, w["vertices"], 1, args.ref_sgns_words, walkers=walkers, timeout=args.ref_timeout)
     if not (res and res["rounds"] and res["sgns_train_s"]):
         return {"unavailable": "oracle/_ref/ref_embed missing or failed"}
@@ -850,8 +821,6 @@ def main():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")
     ap.add_argument("--ref-sgns-words", type=int, default=1_000_000)
-    ap.add_argument("--ref-walkers", type=int, default=100_000,
-                    help="walkers of each of the reference's sampled walk rounds (a prefix of the walker ids)")
     ap.add_argument("--auc", action="store_true",
                     help="run the whole embedding job on a 10%%-held-out split and print link-prediction AUC lines")
     ap.add_argument("--workload", choices=["c1_small", "c2_youtube", "c3_livejournal", "c5_twitter",

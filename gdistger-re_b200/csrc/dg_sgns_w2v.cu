@@ -384,6 +384,14 @@ static int resident_blocks(K kern, int threads, size_t smem, int device) {
     return std::max(per_sm, 1) * dg::sm_count(device);
 }
 
+// Threads per block: one warp in deterministic mode; a worker count below a
+// block's eight warps is one block of that many warps.
+static int w2v_threads(const dg_sgns *s) {
+    if (s->p.deterministic) return 32;
+    if (s->p.workers > 0 && s->p.workers < (uint32_t)(kW2vThreads / 32)) return 32 * (int)s->p.workers;
+    return kW2vThreads;
+}
+
 static int worker_blocks(const dg_sgns *s, int resident, int threads) {
     if (s->p.workers == 0) return resident;
     const int want = (int)((s->p.workers + threads / 32 - 1) / (threads / 32));
@@ -394,7 +402,7 @@ template <int V>
 static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     constexpr int G = V <= 4 ? 6 : 2;
     auto kern = sgns_cbow_kernel<V, G>;
-    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int threads = w2v_threads(s);
     const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
     kern<<<blocks, threads, 0, s->stream>>>(a, ws);
     dg::note_launch();
@@ -405,7 +413,7 @@ static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 template <int V>
 static int negshare_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     auto kern = sgns_negshare_kernel<V>;
-    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int threads = w2v_threads(s);
     const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
     kern<<<blocks, threads, 0, s->stream>>>(a, ws);
     dg::note_launch();
@@ -427,7 +435,7 @@ int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 template <int V>
 static int plain_hs_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
     auto kern = sgns_plain_hs_kernel<V>;
-    const int threads = s->p.deterministic ? 32 : kW2vThreads;
+    const int threads = w2v_threads(s);
     const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
     kern<<<blocks, threads, 0, s->stream>>>(a, ws);
     dg::note_launch();

@@ -59,10 +59,10 @@ constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
 // as many): enough residency to reach the staleness bound on large vocabularies.
 constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 5 : 3; }
 // Register cap per thread: what mb_min_blocks workers per SM leave (size 128:
-// 200, which five 64-thread workers fit and which keeps the step free of
-// spills; shared memory holds five of them too).
+// 192, so that five 64-thread workers fit the register file, as many as shared
+// memory holds, and the step still spills nothing).
 constexpr int mb_max_regs(int d) {
-    return d == 128 ? 200 : (65536 / (32 * mb_warps(d) * mb_min_blocks(d)) > 255 ? 255
+    return d == 128 ? 192 : (65536 / (32 * mb_warps(d) * mb_min_blocks(d)) > 255 ? 255
                                  : 65536 / (32 * mb_warps(d) * mb_min_blocks(d)) / 8 * 8);
 }
 

@@ -348,7 +348,8 @@ def measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=Fal
     v_num = w["vertices"]
     sgns = SGNS(v_num, counts, size=w["size"], window=w["window"], negative=w["negative"], batch_size=21,
                 sample=w["sample"], alpha=w["alpha"], iter=w["iter"], min_count=w["min_count"], mode=form,
-                seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local)
+                seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local,
+                master_rows=args.master_rows if form in ("plain_bf16", "minibatch") else 0)
     wp = _lib.WalkParams(min_len=w["min_L"], init_round=w["min_R"], walker_num=v_num, max_len=w["max_len"],
                          seed=2024 + rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
@@ -517,7 +518,7 @@ def run_ours(args, rank, world, local, pg):
     counts = out_deg + in_deg              # word2vec vocabulary from degrees (huge_walk.cpp:43-46)
 
     acc, sgns, wp = measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=True)
-    e2e_value, h2d, d2h = measure_e2e(args, graph, sgns, wp, v_num, w["max_len"], pg)
+    e2e_value, h2d, d2h = (None, 0, 0) if args.no_e2e else measure_e2e(args, graph, sgns, wp, v_num, w["max_len"], pg)
     sgns.close()
     roof = roofline(wl, form, acc, args)
     # FP32 plain (word2vec.cu's skip_gram_kernel rule) on the same graph, beside the headline form.
@@ -538,6 +539,8 @@ def run_ours(args, rank, world, local, pg):
             cpu = cpu_baseline(args, wl, graph, host_edges)
         cfg = {k: v for k, v in w.items() if k not in ("headline", "source")}
         cfg.update(einfo)
+        if form in ("plain_bf16", "minibatch"):
+            cfg["master_rows"] = args.master_rows or 65536
         cfg.update(workload=f"{wl}_{form}" + ("_adjoint" if args.adjoint else ""), sgns_form=form,
                    walkers_per_round=v_num, l2="flushed between steps (256 MB write); rows and CSR exceed L2",
                    parallelism=f"replicas x{world}")
@@ -817,6 +820,7 @@ def main():
                     help="trainer form of the bench line (default: the workload's headline form)")
     ap.add_argument("--bench-workload", dest="workload_bench", choices=sorted(BENCH), default="c5_twitter")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the FP32 plain measurement beside the headline")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer (e2e) measurement (experiments only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     ap.add_argument("--adjoint", action="store_true", help="train by adjoint gradient steps (deterministic mode 2)")
@@ -834,7 +838,8 @@ def main():
                     help="AUC runs: launch shape of the plain kernel (an index of the autotuner's list)")
     ap.add_argument("--workers", default="", help="--auc: comma-separated trainer worker counts to sweep (0 = auto)")
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--master-rows", type=int, default=0, help="--auc: FP32 master rows of the minibatch form")
+    ap.add_argument("--master-rows", type=int, default=0,
+                    help="FP32 master rows (hottest words) of the BF16 forms; 0 = 65,536")
     ap.add_argument("--tmpdir", default=None)
     ap.add_argument("--ref-timeout", type=int, default=7200)
     args = ap.parse_args()

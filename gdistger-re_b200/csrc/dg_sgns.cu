@@ -491,7 +491,8 @@ struct BfRows {
             r.v[1] = __uint_as_float(t & 0xFFFF0000u);
         }
     }
-    // One hash per row write; each 32-bit word of noise rounds two elements (low
+    // One multiply-xorshift of the salt per row write (the salts already differ
+    // by row, pair and lane); each 32-bit word of noise rounds two elements (low
     // half for the even element, high half for the odd one), the next word comes
     // from one LCG step.  The rounding is bf16_sr_bits, done by the stochastic-
     // rounding convert (cvt.rs.bf16x2.f32: upper result = a rounded with
@@ -499,7 +500,8 @@ struct BfRows {
     // result for every non-NaN input (infinities kept; a NaN stays a NaN).
     __device__ __forceinline__ void store_bits(int32_t w, uint32_t lane, const RowVec<VEC> &r, uint32_t salt) const {
         uint32_t word[VEC / 2];
-        uint32_t x = bf_mix(salt);
+        uint32_t x = salt * 0x9E3779B1u;
+        x ^= x >> 16;
 #pragma unroll
         for (int i = 0; i < VEC; i += 2) {
             asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(word[i / 2]) : "f"(r.v[i + 1]), "f"(r.v[i]), "r"(x));

@@ -18,7 +18,8 @@
  *    atomics); a BF16 row is overwritten with the warp's updated copy, rounded
  *    stochastically: 16 noise bits added below the kept mantissa, then
  *    truncated, the noise words drawn per row write from a salt exactly as the
- *    kernel's BfRows::store_bits does.  Infinities and NaN are not expected.
+ *    kernel's BfRows::store_bits does (one multiply-xorshift of the salt, then
+ *    one LCG step per two elements).  Infinities and NaN are not expected.
  */
 #include "dg_oracle.h"
 #include "philox.h"
@@ -86,7 +87,8 @@ static void row_update(const dgo_pipe_cfg *c, float *row, int32_t id, const floa
         return;
     }
     for (int l = 0; l < 32; l++) {
-        uint32_t x = bf_mix(salt[l]);
+        uint32_t x = salt[l] * 0x9E3779B1u;   /* the kernel's per-write noise word */
+        x ^= x >> 16;
         for (int i = 0; i < v; i += 2) {
             row[l * v + i] = bf16_sr(value[l * v + i], x & 0xFFFFu);
             row[l * v + i + 1] = bf16_sr(value[l * v + i + 1], x >> 16);

@@ -90,6 +90,27 @@ def test_huge_walk_reference_defaults(distger_lib, oracle, tmp_path):
     np.testing.assert_allclose(got[ids], _by_vertex(o, 200)[ids], atol=6e-7, rtol=0)
 
 
+def test_huge_walk_run_sh_flags(distger_lib, tmp_path):
+    """The reference's run.sh learning flags (build/run.sh:60-71) verbatim, on the
+    tiny graph: -size 100 (stored padded to 128 columns), -iter 3, -threads 10,
+    -sync-size 1024; CBOW by default.  The embedding has 100 columns."""
+    from distger import lp
+    edges_path = os.path.join(GOLDEN, "tiny200.bin")
+    emb_path = str(tmp_path / "emb.txt")
+    out = _run(["-g", edges_path, "-v", "200", "-w", "200", "--min_L", "20", "--min_R", "1", "-o",
+                str(tmp_path / "walks"), "--make-undirected", "-emb_output", emb_path, "-size", "100", "-iter", "3",
+                "-threads", "10", "-window", "10", "-negative", "5", "-batch-size", "21", "-min-count", "0",
+                "-sample", "1e-3", "-alpha", "0.01", "-debug", "2", "-sync-size", "1024", "-rounds", "4",
+                "-table-size", "100000"])
+    assert "mode cbow" in out
+    with open(emb_path) as f:
+        assert f.readline().split() == ["200", "100"]
+        row = f.readline().split()
+    assert len(row) == 101
+    emb = lp.read_embedding_text(emb_path, 200)
+    assert emb.shape == (200, 100) and np.isfinite(emb).all() and np.abs(emb).max() > 0
+
+
 def test_huge_walk_rejects_bad_flags():
     r = subprocess.run([EXE, "-g", "x.bin", "-v", "10", "-w", "10", "-binary", "1"], capture_output=True, text=True)
     assert r.returncode == 2 and "not supported" in r.stderr

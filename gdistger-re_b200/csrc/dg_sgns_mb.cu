@@ -59,8 +59,9 @@ constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
 // as many): enough residency to reach the staleness bound on large vocabularies.
 constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 5 : 3; }
 // Register cap per thread: what mb_min_blocks workers per SM leave (size 128:
-// 192, so that five 64-thread workers fit the register file, as many as shared
-// memory holds, and the step still spills nothing).
+// 192, four 64-thread workers per SM -- a warp's registers come from one SM
+// sub-partition's 16,384 -- with no spills; 168, which five workers would
+// need, spills).
 constexpr int mb_max_regs(int d) {
     return d == 128 ? 192 : (65536 / (32 * mb_warps(d) * mb_min_blocks(d)) > 255 ? 255
                                  : 65536 / (32 * mb_warps(d) * mb_min_blocks(d)) / 8 * 8);
@@ -218,6 +219,8 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
     const int window = a.window, negative = a.negative;
 
     // Worker state, identical in every thread.
+    // Indexed only by constants (the loops over the two sentences are unrolled),
+    // so these stay in registers rather than in a local-memory stack frame.
     int len[2] = {0, 0}, pos[2] = {0, 0};
     int nbn = 1;
     unsigned long long n_words = 0, n_trained = 0, n_pairs = 0, n_rows = 0;
@@ -275,6 +278,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
 
     for (;;) {
         // ---- fill empty sentence slots (dsgl.hpp:903-1028); warp 0 builds, all load ----
+#pragma unroll
         for (int s = 0; s < 2; s++) {
             while (len[s] == 0 && next_walk < w_end) {
                 const uint32_t walk = next_walk++;
@@ -417,6 +421,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
         if (warp == 0) {
             const uint32_t b = philox4x32_10(make_uint4(step, worker, 0, kMbWinTag), key0, key1).x % (uint32_t)window;
             int ni = 0;
+#pragma unroll
             for (int s = 0; s < 2; s++) {
                 for (int base = (int)b; base < 2 * window + 1 - (int)b; base += 32) {
                     const int i = base + lane;
@@ -596,6 +601,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
         step++;
         pos[0]++;
         pos[1]++;
+#pragma unroll
         for (int s = 0; s < 2; s++)
             if (pos[s] >= len[s]) {
                 flush_sentence(s);
@@ -612,6 +618,7 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
     }
     // Slice exhausted: keep the updates of the sentence still in flight and of
     // the pool (dsgl drops them; here they are written back).
+#pragma unroll
     for (int s = 0; s < 2; s++)
         if (len[s] != 0) flush_sentence(s);
     if (pool_loaded) flush_pool();

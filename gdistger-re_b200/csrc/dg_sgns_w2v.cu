@@ -78,10 +78,16 @@ __device__ __forceinline__ void hs_path(const SgnsArgs &a, int32_t word, const R
 
 // ------------------------------------------------------------------ CBOW
 
+// Blocks per SM the CBOW kernel's registers are capped for: the kernel waits on
+// row gathers, so residency pays (size 128, YouTube-shaped vocabulary: 44.8 ms
+// per pass at four 256-thread blocks and three target rows in flight, 64.8 ms
+// at two blocks and six rows).
+constexpr int cbow_min_blocks(int vec) { return vec <= 4 ? 4 : 1; }
+
 // G: target rows fetched together (their loads overlap); later groups are
 // fetched after the earlier ones are written.
 template <int VEC, int G>
-__global__ void __launch_bounds__(kW2vThreads) sgns_cbow_kernel(SgnsArgs a, WalkSet ws) {
+__global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
     const uint32_t lane = threadIdx.x & 31;
     int32_t *sen = sen_all[threadIdx.x >> 5];
@@ -400,7 +406,7 @@ static int worker_blocks(const dg_sgns *s, int resident, int threads) {
 
 template <int V>
 static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    constexpr int G = V <= 4 ? 6 : 2;
+    constexpr int G = V == 4 ? 3 : V <= 2 ? 4 : 2;
     auto kern = sgns_cbow_kernel<V, G>;
     const int threads = w2v_threads(s);
     const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);

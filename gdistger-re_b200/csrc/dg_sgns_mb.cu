@@ -58,13 +58,14 @@ constexpr int mb_warps(int d) { return d >= 64 ? d / 64 : 1; }
 // Workers per SM the register budget is sized for (shared memory allows about
 // as many): enough residency to reach the staleness bound on large vocabularies.
 constexpr int mb_min_blocks(int d) { return d <= 32 ? 16 : d == 64 ? 8 : d == 128 ? 5 : 3; }
-// Register cap per thread: what mb_min_blocks workers per SM leave (size 128:
-// 192, four 64-thread workers per SM -- a warp's registers come from one SM
-// sub-partition's 16,384 -- with no spills; 168, which five workers would
-// need, spills).
+// Register cap per thread: the most that mb_min_blocks workers per SM leave.
+// Registers are allocated per SM sub-partition (four per SM, 16,384 each), so
+// the cap is 16,384 / (32 x the warps one sub-partition holds); size 128: five
+// two-warp workers, three warps per sub-partition, 168 registers.
 constexpr int mb_max_regs(int d) {
-    return d == 128 ? 192 : (65536 / (32 * mb_warps(d) * mb_min_blocks(d)) > 255 ? 255
-                                 : 65536 / (32 * mb_warps(d) * mb_min_blocks(d)) / 8 * 8);
+    return 16384 / (32 * ((mb_warps(d) * mb_min_blocks(d) + 3) / 4)) / 8 * 8 > 255
+               ? 255
+               : 16384 / (32 * ((mb_warps(d) * mb_min_blocks(d) + 3) / 4)) / 8 * 8;
 }
 
 __device__ __forceinline__ uint32_t mix32(uint32_t h) {
@@ -185,7 +186,9 @@ __global__ void __launch_bounds__(32 * mb_warps(D)) __maxnreg__(mb_max_regs(D)) 
     constexpr int NW = mb_warps(D);
     constexpr int V = D / (32 * NW);
     constexpr int IPB = 32 / OUT;                   // inputs per batch of 32 corr dots
-    constexpr int kRowBatch = 8;                    // rows whose loads are issued together
+    // Rows whose loads are issued together by the fills and flushes (4: the
+    // step fits the 168-register cap without spilling; 8 needed 192).
+    constexpr int kRowBatch = 4;
     extern __shared__ __align__(16) float smem[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int col = warp * 32 * V + lane * V;

@@ -1,11 +1,15 @@
 """Link-prediction split and AUC scoring for the embeddings.
 
-Split: the hold-out rule of the reference's gtrain tool (src/tools/gtrain.cpp:
-226-386): `frac * |E|` edges are removed one at a time, each drawn uniformly
-from the remaining edges and accepted only while both endpoints keep an
-(undirected) degree above 1 in the shrinking graph; the same number of negative
-pairs are drawn uniformly among vertex pairs that are neither edges of the full
-graph nor already drawn.  Seeded here (gtrain seeds with time(0)).
+Split: the reference's gtrain tool (src/tools/gtrain.cpp:226-386) step for
+step, with its random stream: the C library's rand() seeded by srand(seed)
+(gtrain seeds with time(0); given that seed the split here is the tool's, edge
+for edge and in the same order).  npos = (float) frac * |E| edges are removed
+one at a time: an index is drawn among the edges not yet removed (get_big_rand)
+until both endpoints have an (undirected) degree above 1, the edge is taken,
+both degrees drop by one and the edge is swapped with the last one kept.  As
+many negative pairs are drawn (source, then destination, each get_big_rand over
+the vertices) until the pair is not an edge of the full graph in either
+direction and not a pair already drawn in that direction.
 
 Score: sigmoid of the dot product of the two vertices' input embeddings
 (cosine reported too); AUC as the Mann-Whitney rank statistic with ties
@@ -13,54 +17,83 @@ averaged.  The reference ships no scorer; this one is used for every run.
 """
 from __future__ import annotations
 
+import ctypes
+import ctypes.util
+
 import numpy as np
 
+RAND_MAX = 2147483647   # the C library's (glibc) RAND_MAX, which gtrain's get_big_rand assumes
 
-def split(edges: np.ndarray, v_num: int, frac: float = 0.1, seed: int = 2):
-    """Returns (train_edges, test_pairs int64[n, 2], test_labels int8[n])."""
-    rng = np.random.default_rng(seed)
-    src = edges["src"].astype(np.int64)
-    dst = edges["dst"].astype(np.int64)
-    m = src.size
-    npos = int(frac * m)
-    deg = np.bincount(src, minlength=v_num) + np.bincount(dst, minlength=v_num)
-    held = np.zeros(m, dtype=bool)
-    order = rng.permutation(m)
-    taken = 0
-    deg_l = deg.tolist()
-    for e in order.tolist():
-        if taken == npos:
-            break
-        s, d = int(src[e]), int(dst[e])
-        if deg_l[s] <= 1 or deg_l[d] <= 1:
-            continue
-        deg_l[s] -= 1
-        deg_l[d] -= 1
-        held[e] = True
-        taken += 1
-    pos = np.stack([src[held], dst[held]], axis=1)
-    # Negatives: uniform pairs that are not edges (either direction) and not repeated.
-    key = lambda a, b: np.minimum(a, b) * v_num + np.maximum(a, b)  # noqa: E731
-    existing = set(key(src, dst).tolist())
-    chosen = set()
+
+def _libc():
+    return ctypes.CDLL(ctypes.util.find_library("c") or "libc.so.6")
+
+
+def _big_rand(rand, rng: int) -> int:
+    """gtrain.cpp:214-223 (get_big_rand), including its quirks: for ranges of
+    RAND_MAX and more it never returns a value below RAND_MAX."""
+    if rng < RAND_MAX:
+        return rand() % rng
+    rounds, mod = rng // RAND_MAX, rng % RAND_MAX
+    t = rand() % rounds + 1
+    if t == rounds:
+        return t * RAND_MAX + rand() % mod
+    return t * RAND_MAX + rand() % RAND_MAX
+
+
+def split(edges: np.ndarray, v_num: int, frac: float = 0.1, seed: int = 2, max_tries: int = 1 << 26):
+    """Returns (train_edges in gtrain's output order, test_pairs int64[n, 2],
+    test_labels int8[n]): positives first, in the order drawn, then negatives.
+    Raises RuntimeError where gtrain would loop forever (no edge left whose
+    endpoints both keep a second edge, or no free vertex pair)."""
+    c = _libc()
+    c.srand.argtypes = [ctypes.c_uint]
+    c.rand.restype = ctypes.c_int
+    c.srand(ctypes.c_uint(seed & 0xFFFFFFFF))
+    rand = c.rand
+    src = edges["src"].astype(np.int64).tolist()
+    dst = edges["dst"].astype(np.int64).tolist()
+    order = list(range(len(src)))          # edges[] of the tool, permuted by its swaps
+    m = len(src)
+    npos = int(np.float32(frac) * np.float32(m))   # float * size_t in the tool
+    deg = (np.bincount(edges["src"], minlength=v_num) + np.bincount(edges["dst"], minlength=v_num)).tolist()
+    pos = []
+    tail = m - 1
+    tries = 0
+    for _ in range(npos):
+        ep = _big_rand(rand, tail + 1)
+        while deg[src[order[ep]]] <= 1 or deg[dst[order[ep]]] <= 1:
+            tries += 1
+            if tries > max_tries:
+                raise RuntimeError("split: no edge left whose endpoints both keep a second edge")
+            ep = _big_rand(rand, tail + 1)
+        e = order[ep]
+        pos.append((src[e], dst[e]))
+        deg[src[e]] -= 1
+        deg[dst[e]] -= 1
+        order[ep], order[tail] = order[tail], order[ep]
+        tail -= 1
+    # Negatives (gtrain.cpp:328-342): not an edge of the full graph (its CSR has
+    # both directions), not drawn before as the same (source, destination).
+    existing = set((a * v_num + b) for a, b in zip(src, dst))
+    existing.update(b * v_num + a for a, b in zip(src, dst))
+    drawn = set()
     neg = []
-    while len(neg) < taken:
-        a = rng.integers(0, v_num, size=2 * (taken - len(neg)) + 16)
-        b = rng.integers(0, v_num, size=a.size)
-        for x, y in zip(a.tolist(), b.tolist()):
-            if x == y:
-                continue
-            k = min(x, y) * v_num + max(x, y)
-            if k in existing or k in chosen:
-                continue
-            chosen.add(k)
-            neg.append((x, y))
-            if len(neg) == taken:
+    for _ in range(npos):
+        while True:
+            a = _big_rand(rand, v_num)
+            b = _big_rand(rand, v_num)
+            k = a * v_num + b
+            if k not in existing and k not in drawn:
                 break
-    neg = np.array(neg, dtype=np.int64).reshape(-1, 2)
-    pairs = np.concatenate([pos, neg])
+            tries += 1
+            if tries > max_tries:
+                raise RuntimeError("split: no free vertex pair left for a negative")
+        drawn.add(k)
+        neg.append((a, b))
+    pairs = np.array(pos + neg, dtype=np.int64).reshape(-1, 2)
     labels = np.concatenate([np.ones(len(pos), np.int8), np.zeros(len(neg), np.int8)])
-    return edges[~held], pairs, labels
+    return edges[np.array(order[:tail + 1], dtype=np.int64)], pairs, labels
 
 
 def auc(scores: np.ndarray, labels: np.ndarray) -> float:

@@ -1,10 +1,59 @@
 """Link-prediction split and AUC scorer (CPU).
 
-The split follows the hold-out rule of src/tools/gtrain.cpp:226-386; the AUC is
-checked against scikit-learn's roc_auc_score, ties included.
+The split is src/tools/gtrain.cpp:226-386 with the tool's random stream: given
+the seed that the tool takes from time(0), its three output files are
+reproduced byte for byte -- against digests of the unmodified tool's output
+(tests/golden/gtrain_ref.json, tests/golden/make_gtrain_golden.py) and, where
+oracle/_ref holds the tool, against a live run of it.  The AUC is checked
+against scikit-learn's roc_auc_score, ties included.
 """
+import hashlib
+import json
+import os
+import sys
+
 import numpy as np
 import pytest
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+GTRAIN = os.path.join(os.path.dirname(GOLDEN), "..", "oracle", "_ref", "gtrain_ref")
+
+
+def _golden_cases():
+    sys.path.insert(0, GOLDEN)
+    import make_gtrain_golden
+    return make_gtrain_golden
+
+
+def _split_files(edges, v, frac, seed):
+    """lp.split's result in the tool's three output formats (gtrain.cpp:344-385)."""
+    from distger import lp
+    train, pairs, labels = lp.split(edges, v, frac=frac, seed=seed)
+    lpt = "".join(f"{a} {b} {c}\n" for a, b, c in
+                  zip(train["src"].tolist(), train["dst"].tolist(), train["data"].astype(np.int64).tolist()))
+    te = "".join(f"{a} {b}\n" for a, b in pairs.tolist())
+    tl = "".join(f"{x}\n" for x in labels.tolist())
+    return [lpt.encode(), te.encode(), tl.encode()]
+
+
+@pytest.mark.parametrize("name", ["small", "mid", "dense_holdout"])
+def test_split_reproduces_gtrain_golden(name):
+    g = _golden_cases()
+    with open(os.path.join(GOLDEN, "gtrain_ref.json")) as f:
+        ref = json.load(f)[name]
+    n, _, _, seed, frac = g.CASES[name]
+    files = _split_files(g.case_edges(name), n, frac, seed)
+    assert [f.count(b"\n") for f in files] == ref["lines"]
+    assert [hashlib.sha256(f).hexdigest() for f in files] == ref["sha256"]
+
+
+@pytest.mark.skipif(not os.path.exists(GTRAIN), reason="reference gtrain not built here (make -C oracle ref)")
+@pytest.mark.parametrize("name", ["small", "dense_holdout"])
+def test_split_reproduces_gtrain_live(name, tmp_path):
+    g = _golden_cases()
+    n, _, _, seed, frac = g.CASES[name]
+    want = g.run_ref(name, str(tmp_path))
+    assert _split_files(g.case_edges(name), n, frac, seed) == want
 
 
 def test_auc_matches_sklearn():
@@ -62,8 +111,9 @@ def test_split_positives_are_edges_and_negatives_are_not(c1_split):
     assert all(k in all_keys and k not in train_keys for k in pk[:npos].tolist())
     neg = pk[npos:].tolist()
     assert not any(k in all_keys for k in neg)
-    assert len(set(neg)) == len(neg)
-    assert np.all(pairs[npos:, 0] != pairs[npos:, 1])
+    # gtrain rejects a pair drawn before in the same direction only (gtrain.cpp:202-211).
+    directed = (pairs[npos:, 0] * v + pairs[npos:, 1]).tolist()
+    assert len(set(directed)) == len(directed)
 
 
 def test_split_is_seeded(c1_split):

@@ -168,14 +168,14 @@ __global__ void init_rows_f32(float *rows, uint64_t n, int d, int dp) {
             continue;
         }
         const unsigned long long x = lcg_state(r * (uint64_t)d + c);
-        rows[k] = (((x & 0xFFFF) / (float)65536) - 0.5f) / d;
+        rows[k] = (float)(((double)((x & 0xFFFF) / (float)65536) - 0.5) / (double)d);   // double, as word2vec.cu:872
     }
 }
 
 __global__ void init_rows_bf16(__nv_bfloat16 *rows, float *master, uint64_t n, uint64_t n_master, int d) {
     for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (uint64_t)gridDim.x * blockDim.x) {
         const unsigned long long x = lcg_state(k);
-        const float v = (((x & 0xFFFF) / (float)65536) - 0.5f) / d;
+        const float v = (float)(((double)((x & 0xFFFF) / (float)65536) - 0.5) / (double)d);
         rows[k] = __float2bfloat16_rn(v);
         if (k < n_master) master[k] = v;
     }

@@ -100,7 +100,8 @@ void dgo_init_rows(uint32_t vocab_size, int d, float *syn0) {
     for (uint64_t a = 0; a < vocab_size; a++)
         for (int b = 0; b < d; b++) {
             next_random = next_random * (unsigned long long)25214903917ULL + 11;
-            syn0[a * d + b] = (((next_random & 0xFFFF) / (float)65536) - 0.5f) / d;
+            /* 0.5 and layer1_size promote the expression to double; the result is rounded to float */
+            syn0[a * d + b] = (float)(((double)((next_random & 0xFFFF) / (float)65536) - 0.5) / (double)d);
         }
 }
 

@@ -12,7 +12,9 @@
  * with reduSize computed as TrainModelThread computes it (word2vec.cu:971-973).
  * All pointers are device pointers owned by the caller; the table must hold
  * the reference's fixed table_size (1e8, word2vec.cu:66) entries.
- * ref_w2v_huffman() runs the reference's host-side Huffman coding.
+ * ref_w2v_huffman() runs the reference's host-side Huffman coding;
+ * ref_w2v_vocab(), ref_w2v_unigram() and ref_w2v_init_rows() its vocabulary,
+ * unigram table and initial rows.
  */
 #include "word2vec.cu"
 
@@ -77,5 +79,66 @@ int ref_w2v_huffman(const long long *cn, long long n, int *codelen_out, int *poi
 
 /* The reference's fixed unigram-table size (word2vec.cu:66). */
 int ref_w2v_table_size(void) { return table_size; }
+
+/* The reference's vocabulary from vertex degrees: ReadVocabFromDegree
+ * (word2vec.cu:791-809; word = the vertex id as text, count = its degree) with
+ * SortVocab (word2vec.cu:629-659: the C library's qsort by count, min_count cut,
+ * train_words), after main's allocations (word2vec.cu:1569-1570).  Host code, no
+ * GPU.  Writes, in vocabulary order, each word's vertex id and count (at most
+ * cap entries), the vocabulary size and train_words.  The vocabulary stays in
+ * place for ref_w2v_unigram and ref_w2v_init_rows.  Returns 0, or -1 when cap
+ * is smaller than the vocabulary. */
+int ref_w2v_vocab(const unsigned *deg, unsigned v_num, int min_cnt, long long cap, unsigned *id_out,
+                  long long *cn_out, long long *size_out, long long *train_words_out) {
+    min_count = min_cnt;
+    vocab_max_size = 1000;
+    vocab_size = 0;
+    vocab = (struct vocab_word *)calloc(vocab_max_size, sizeof(struct vocab_word));
+    if (!vocab_hash) vocab_hash = (int *)calloc(vocab_hash_size, sizeof(int));
+    std::vector<vertex_id_t> degrees(deg, deg + v_num);
+    ReadVocabFromDegree(degrees);
+    *size_out = vocab_size;
+    *train_words_out = train_words;
+    if (vocab_size > cap) return -1;
+    for (long long a = 0; a < vocab_size; a++) {
+        id_out[a] = (unsigned)strtoul(vocab[a].word, nullptr, 10);
+        cn_out[a] = vocab[a].cn;
+    }
+    return 0;
+}
+
+/* InitUnigramTable (word2vec.cu:537-556) over the vocabulary of the last
+ * ref_w2v_vocab call; copies its host table (table_size entries) to table_out.
+ * Needs a GPU (the function also uploads the table).  Returns 0 or the CUDA
+ * error code. */
+int ref_w2v_unigram(int *table_out) {
+    InitUnigramTable();
+    memcpy(table_out, table, (size_t)table_size * sizeof(int));
+    free(table);
+    table = nullptr;
+    cudaFree(d_table);
+    d_table = nullptr;
+    return (int)cudaGetLastError();
+}
+
+/* InitNet (word2vec.cu:844-878) for the last vocabulary with d columns and
+ * negative sampling: copies the host syn0 (vocab_size x d, the LCG-initialised
+ * input rows) to rows_out.  Needs a GPU (InitNet uploads the rows and the
+ * Huffman codes).  Returns 0 or the CUDA error code. */
+int ref_w2v_init_rows(int d, float *rows_out) {
+    layer1_size = d;
+    negative = 5;
+    hs = 0;
+    InitNet();
+    memcpy(rows_out, syn0, (size_t)vocab_size * d * sizeof(float));
+    free(syn0);
+    free(syn1neg);
+    free(last_emb);
+    syn0 = syn1neg = last_emb = nullptr;
+    cudaFree(d_syn0);
+    cudaFree(d_syn1);
+    d_syn0 = d_syn1 = nullptr;
+    return (int)cudaGetLastError();
+}
 
 }  // extern "C"

@@ -56,3 +56,39 @@ def test_negreuse_within_tolerance(exp_tab):
     np.testing.assert_allclose(m1, r1, rtol=1e-5, atol=2e-6)
     x0, _ = W.run_restatement(c, table, exp_tab, exact_sum=1)
     assert np.abs(x0 - r0).max() > 100 * np.abs(m0 - r0).max() + 1e-3
+
+
+@pytest.mark.parametrize("name,size", [("tiny200_mc5", 128), ("cl10k_mc0", 128), ("cl10k_mc0", 100)])
+def test_vocab_unigram_table_and_initial_rows_match_reference(distger_lib, name, size):
+    """The library's vocabulary, unigram table (the reference's 1e8 slots) and
+    initial input rows (size 100 stored padded to 128) equal word2vec.cu's own ReadVocabFromDegree + SortVocab,
+    InitUnigramTable and InitNet (word2vec.cu:537-556, 791-809, 844-878) run from
+    oracle/_ref/libref_w2v.so, bit for bit."""
+    import ctypes as C
+    import sys
+
+    import dgoracle
+    from distger.sgns import SGNS
+    _lib_or_skip()
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden"))
+    import make_vocab_golden as g
+    counts = g.case_counts(name)
+    min_count = g.CASES[name][4]
+    ids, cn, tw = g.ref_vocab(counts, min_count)
+    L = C.CDLL(dgoracle.REF_W2V)
+    L.ref_w2v_unigram.argtypes = [C.c_void_p]
+    L.ref_w2v_init_rows.argtypes = [C.c_int, C.c_void_p]
+    table = np.zeros(L.ref_w2v_table_size(), np.int32)
+    assert L.ref_w2v_unigram(table.ctypes.data) == 0
+    rows_ref = np.zeros((ids.size, size), np.float32)
+    assert L.ref_w2v_init_rows(size, rows_ref.ctypes.data) == 0
+    s = SGNS(counts.size, counts, size=size, window=5, negative=5, sample=1e-3, min_count=min_count, mode="plain",
+             seed=1, table_size=0)
+    rows, vids = s.embedding()
+    np.testing.assert_array_equal(vids, ids)
+    assert s.train_words == tw
+    t = s.tables()
+    assert t["table"].size == table.size
+    np.testing.assert_array_equal(t["table"], table)
+    assert np.array_equal(rows.view(np.uint32), rows_ref.view(np.uint32))
+    s.close()

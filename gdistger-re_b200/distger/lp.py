@@ -96,6 +96,20 @@ def split(edges: np.ndarray, v_num: int, frac: float = 0.1, seed: int = 2, max_t
     return edges[np.array(order[:tail + 1], dtype=np.int64)], pairs, labels
 
 
+def write_split(train: np.ndarray, pairs: np.ndarray, labels: np.ndarray, lpfile: str, test_edges: str,
+                test_labels: str) -> None:
+    """Writes split()'s result as gtrain writes it (gtrain.cpp:344-385): the
+    train edges as `src dst data` lines (data as an unsigned integer), the test
+    pairs as `src dst` lines, the labels one per line."""
+    with open(lpfile, "w") as f:
+        f.writelines(f"{a} {b} {c}\n" for a, b, c in
+                     zip(train["src"].tolist(), train["dst"].tolist(), train["data"].astype(np.int64).tolist()))
+    with open(test_edges, "w") as f:
+        f.writelines(f"{a} {b}\n" for a, b in pairs.tolist())
+    with open(test_labels, "w") as f:
+        f.writelines(f"{x}\n" for x in labels.tolist())
+
+
 def auc(scores: np.ndarray, labels: np.ndarray) -> float:
     """Area under the ROC curve (Mann-Whitney U / (n_pos * n_neg)), ties averaged."""
     scores = np.asarray(scores, dtype=np.float64)

@@ -26,14 +26,15 @@ def _golden_cases():
 
 
 def _split_files(edges, v, frac, seed):
-    """lp.split's result in the tool's three output formats (gtrain.cpp:344-385)."""
+    """lp.split's result as lp.write_split writes it (the tool's three output formats)."""
+    import tempfile
+
     from distger import lp
     train, pairs, labels = lp.split(edges, v, frac=frac, seed=seed)
-    lpt = "".join(f"{a} {b} {c}\n" for a, b, c in
-                  zip(train["src"].tolist(), train["dst"].tolist(), train["data"].astype(np.int64).tolist()))
-    te = "".join(f"{a} {b}\n" for a, b in pairs.tolist())
-    tl = "".join(f"{x}\n" for x in labels.tolist())
-    return [lpt.encode(), te.encode(), tl.encode()]
+    with tempfile.TemporaryDirectory() as d:
+        paths = [os.path.join(d, x) for x in ("lp.txt", "te.txt", "tl.txt")]
+        lp.write_split(train, pairs, labels, *paths)
+        return [open(p, "rb").read() for p in paths]
 
 
 @pytest.mark.parametrize("name", ["small", "mid", "dense_holdout"])

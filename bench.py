@@ -47,6 +47,8 @@ SGNS_HP = {"size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.
 # leaving ~1.47e9 unique undirected edges, unweighted; --min_R 5 (run.sh:45), walks
 # of at most 32 footprints; headline form: BF16 rows with FP32 masters (the plain
 # rule), FP32 plain beside it.  c2_youtube: the YouTube-shaped graph, FP32 plain.
+# c3_livejournal: the LiveJournal-shaped graph (2,238,731 vertices, exponent 2.3,
+# 14M undirected edge draws, weighted), BF16 rows against FP32 plain.
 BENCH = {
     "c5_twitter": dict(graph="twitter-shaped chung-lu, generated on the device", source="device",
                        vertices=41_652_230, draws=2_417_000_000, exponent=1.9, max_degree=3_000_000, weighted=False,
@@ -54,6 +56,9 @@ BENCH = {
     "c2_youtube": dict(graph="youtube-shaped chung-lu", source="host", vertices=1_138_499,
                        undirected_edges=2_990_443, exponent=2.1, max_degree=28_000, weighted=True,
                        min_L=20, min_R=10, max_len=64, headline="plain", **SGNS_HP),
+    "c3_livejournal": dict(graph="livejournal-shaped chung-lu", source="host", vertices=2_238_731,
+                           undirected_edges=14_000_000, exponent=2.3, max_degree=None, weighted=True,
+                           min_L=20, min_R=10, max_len=64, headline="plain_bf16", **SGNS_HP),
 }
 WORKLOAD = dict(BENCH["c2_youtube"])   # the reference arm's C2 configuration
 # Algorithmic bytes per unit: plain SGNS pair = the context row and 1 + n output
@@ -151,9 +156,9 @@ def barrier(pg):
         pg.barrier()
 
 
-def make_graph_edges():
+def make_graph_edges(workload: str = "c2_youtube"):
     from distger import graphgen
-    return graphgen.chung_lu(**graphgen.CONFIGS["c2_youtube"])
+    return graphgen.chung_lu(**graphgen.CONFIGS[workload])
 
 
 def ref_baseline(edges_path: str, v_num: int, rounds: int, sgns_words: int, walkers: int = 0, timeout: int = 900):
@@ -215,7 +220,7 @@ def run_reference(args, rank, world, pg):
     from distger import graphgen
     with tempfile.TemporaryDirectory(dir=args.tmpdir) as tmp:
         path = os.path.join(tmp, "g.bin")
-        graphgen.write_edges(path, make_graph_edges())
+        graphgen.write_edges(path, make_graph_edges(wl))
         res = ref_baseline(path, w["vertices"], args.warmup + args.steps, args.ref_sgns_words,
                            timeout=args.ref_timeout)
     if res is None or len(res["rounds"]) < args.warmup + args.steps or not res["sgns_train_s"]:
@@ -301,7 +306,7 @@ def load_traffic():
 def build_bench_graph(workload: str, local: int):
     """The workload's graph as a device CSR.  c5_twitter: generated, deduplicated and
     built on the device (dg_edges_chung_lu, dg_graph_create_from_device_edges);
-    c2_youtube: the numpy generator's records loaded through dg_graph_create_from_edges.
+    c2_youtube, c3_livejournal: the numpy generator's records loaded through dg_graph_create_from_edges.
     Returns (graph, edge info, CSR build ms, host edges or None)."""
     import distger
     w = BENCH[workload]
@@ -317,7 +322,7 @@ def build_bench_graph(workload: str, local: int):
         build_ms = (time.perf_counter() - t0) * 1e3
         e.close()
         return graph, {"undirected_edges": n_edges}, build_ms, None
-    edges = make_graph_edges()
+    edges = make_graph_edges(workload)
     distger.Graph(w["vertices"], edges=edges, make_undirected=True, device=local).close()   # context, module load
     t0 = time.perf_counter()
     graph = distger.Graph(w["vertices"], edges=edges, make_undirected=True, device=local)

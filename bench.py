@@ -41,6 +41,7 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 METRIC = "walk-steps/s + SGNS words/s, end-to-end embed time; BF16 vs FP32 plain at equal AUC"
 UNIT = "walk-steps/s"
+BF16_FORMS = ("plain_bf16", "minibatch", "cbow_bf16")   # trainer forms with BF16 rows and FP32 masters
 SGNS_HP = {"size": 128, "window": 10, "negative": 5, "sample": 1e-3, "alpha": 0.01, "iter": 1, "min_count": 0}
 # Bench workloads.  c5_twitter (the default): the Twitter-shaped graph, 41,652,230
 # vertices, Chung-Lu exponent 1.9, expected degrees capped at 3M, 2.417e9 edge draws
@@ -337,7 +338,7 @@ def torch_sync(local: int):
 
 def sgns_kernel_name(form: str) -> str:
     return {"plain": "sgns_plain", "plain_bf16": "sgns_plain_bf16", "minibatch": "sgns_minibatch",
-            "cbow": "sgns_cbow", "sg_shared": "sgns_sg_shared"}[form]
+            "cbow": "sgns_cbow", "cbow_bf16": "sgns_cbow_bf16", "sg_shared": "sgns_sg_shared"}[form]
 
 
 def measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=False):
@@ -354,7 +355,7 @@ def measure_form(args, form, graph, counts, wl, rank, local, pg, with_clocks=Fal
     sgns = SGNS(v_num, counts, size=w["size"], window=w["window"], negative=w["negative"], batch_size=21,
                 sample=w["sample"], alpha=w["alpha"], iter=w["iter"], min_count=w["min_count"], mode=form,
                 seed=1 + rank, deterministic=2 if args.adjoint else 0, device=local,
-                master_rows=args.master_rows if form in ("plain_bf16", "minibatch") else 0)
+                master_rows=args.master_rows if form in BF16_FORMS else 0)
     wp = _lib.WalkParams(min_len=w["min_L"], init_round=w["min_R"], walker_num=v_num, max_len=w["max_len"],
                          seed=2024 + rank)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")   # 256 MB > L2
@@ -462,10 +463,10 @@ def roofline(wl, form, acc, args):
     d, n = w["size"], w["negative"]
     if acc["train_ms"] >= acc["walk_ms"]:
         kern = sgns_kernel_name(form)
-        e = 2 if form in ("plain_bf16", "minibatch") else 4
+        e = 2 if form in BF16_FORMS else 4
         if form == "minibatch":
             model = acc["rows"] * 2 * d * e
-        elif form == "cbow":
+        elif form in ("cbow", "cbow_bf16"):
             model = None
         elif form == "sg_shared":
             model = acc["pairs"] * 2 * d * e
@@ -544,14 +545,14 @@ def run_ours(args, rank, world, local, pg):
             cpu = cpu_baseline(args, wl, graph, host_edges)
         cfg = {k: v for k, v in w.items() if k not in ("headline", "source")}
         cfg.update(einfo)
-        if form in ("plain_bf16", "minibatch"):
+        if form in BF16_FORMS:
             cfg["master_rows"] = args.master_rows or 65536
         cfg.update(workload=f"{wl}_{form}" + ("_adjoint" if args.adjoint else ""), sgns_form=form,
                    walkers_per_round=v_num, l2="flushed between steps (256 MB write); rows and CSR exceed L2",
                    parallelism=f"replicas x{world}")
         line = {"metric": METRIC, "value": acc["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": acc["t_dev"] * 1e3 / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if form in ("plain", "cbow", "sg_shared") else "bf16",
+                "scaling": "weak", "vs_baseline": None, "dtype": "bf16" if form in BF16_FORMS else "f32",
                 "data": "synthetic", "config": cfg,
                 "walk_steps_per_s": acc["steps"] / (acc["walk_ms"] / 1e3),
                 "sgns_words_per_s": acc["words"] / (acc["train_ms"] / 1e3),
@@ -601,7 +602,7 @@ def run_auc_ours(args, local):
         graph.close()
         m = lp.evaluate(res["embedding"], pairs, labels)
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in ("plain_bf16", "minibatch") else "f32",
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in BF16_FORMS else "f32",
                           "workers": workers or res["workers"], "master_rows": args.master_rows, "auc": m["auc"],
                           "auc_cosine": m["auc_cosine"], "test_pairs": int(labels.size), "rounds": len(res["rounds"]),
                           "embed_device_s": res["device_ms"] / 1e3, "embed_wall_s": res["rounds_wall_s"],
@@ -755,7 +756,7 @@ def run_auc_synth(args, local):
         m = pairs.auc(sgns)
         t5 = time.perf_counter()
         print(json.dumps({"metric": "link-prediction AUC", "impl": "ours", "workload": args.workload,
-                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in ("plain_bf16", "minibatch") else "f32", "workers": res["workers"],
+                          "sgns_form": form, "plain_shape": args.plain_shape, "dtype": "bf16" if mode in BF16_FORMS else "f32", "workers": res["workers"],
                           "master_rows": args.master_rows,
                           "auc": m["auc"], "auc_cosine": m["auc_cosine"], "test_pairs": pairs.n_pos + pairs.n_neg,
                           "vertices": cfg["n"], "undirected_edges": n_edges, "rounds": len(res["rounds"]),
@@ -796,8 +797,8 @@ def run_profile_case(args, local):
     check(L.dg_paths_get_info(p1, C.byref(ri)))
     out = {"case": args.profile, "workload": wl, "walks": walkers, "walk_ms": ri.walk_ms, "draws": ri.draws,
            "footprints": ri.footprints}
-    if args.profile in ("sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "sg_shared"):
-        pmode = {"minibatch": "minibatch", "sgns_bf16": "plain_bf16", "cbow": "cbow",
+    if args.profile in ("sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "cbow_bf16", "sg_shared"):
+        pmode = {"minibatch": "minibatch", "sgns_bf16": "plain_bf16", "cbow": "cbow", "cbow_bf16": "cbow_bf16",
                  "sg_shared": "sg_shared"}.get(args.profile, "plain")
         s = SGNS(v_num, counts, size=w["size"], window=w["window"], negative=w["negative"], batch_size=21,
                  sample=w["sample"], alpha=w["alpha"], iter=1, min_count=0, mode=pmode, seed=1,
@@ -813,7 +814,8 @@ def run_profile_case(args, local):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--profile", choices=["walk", "sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "sg_shared"],
+    ap.add_argument("--profile", choices=["walk", "sgns", "sgns_bf16", "minibatch", "adjoint", "cbow", "cbow_bf16",
+                                          "sg_shared"],
                     default=None, help="run one launch of a kernel for ncu and exit")
     ap.add_argument("--profile-walks", type=int, default=50_000, help="--profile: walkers of the round (0: all)")
     ap.add_argument("--profile-workload", choices=sorted(BENCH), default="c2_youtube")
@@ -821,7 +823,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["plain", "plain_bf16", "minibatch", "cbow", "sg_shared"], default=None,
+    ap.add_argument("--mode", choices=["plain", "plain_bf16", "minibatch", "cbow", "cbow_bf16", "sg_shared"], default=None,
                     help="trainer form of the bench line (default: the workload's headline form)")
     ap.add_argument("--bench-workload", dest="workload_bench", choices=sorted(BENCH), default="c5_twitter")
     ap.add_argument("--no-plain-leg", action="store_true", help="skip the FP32 plain measurement beside the headline")

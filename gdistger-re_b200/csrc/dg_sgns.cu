@@ -438,102 +438,6 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_kernel(
     }
 }
 
-// ---------------------------------------------------- plain rule, BF16 rows
-
-__device__ __forceinline__ uint32_t bf_mix(uint32_t h) {
-    h ^= h >> 16;
-    h *= 0x7FEB352Du;
-    h ^= h >> 15;
-    h *= 0x846CA68Bu;
-    h ^= h >> 16;
-    return h;
-}
-
-// FP32 -> BF16 with stochastic rounding: 16 random bits added below the kept
-// mantissa, then truncation (unbiased in expectation; infinities and NaN kept).
-__device__ __forceinline__ uint16_t bf16_sr_bits(float x, uint32_t noise) {
-    uint32_t u = __float_as_uint(x);
-    if ((u & 0x7F800000u) != 0x7F800000u) u += noise & 0xFFFFu;
-    return (uint16_t)(u >> 16);
-}
-
-// A row of the BF16 tables: FP32 masters for ids < n_master, BF16 otherwise.
-// Lane l owns columns [l*VEC, l*VEC + VEC).
-template <int VEC>
-struct BfRows {
-    __nv_bfloat16 *bf;
-    float *master;
-    uint32_t n_master;
-    int d;
-    __device__ __forceinline__ void load(int32_t w, uint32_t lane, RowVec<VEC> &r) const {
-        if ((uint32_t)w < n_master) {
-            load_row<VEC>(master + (size_t)w * d + lane * VEC, r);
-            return;
-        }
-        const uint16_t *p = reinterpret_cast<const uint16_t *>(bf + (size_t)w * d + lane * VEC);
-        if constexpr (VEC == 8) {
-            const uint4 t = __ldcg(reinterpret_cast<const uint4 *>(p));
-            const uint32_t q[4] = {t.x, t.y, t.z, t.w};
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                r.v[2 * i] = __uint_as_float(q[i] << 16);
-                r.v[2 * i + 1] = __uint_as_float(q[i] & 0xFFFF0000u);
-            }
-        } else if constexpr (VEC == 4) {
-            const uint2 t = __ldcg(reinterpret_cast<const uint2 *>(p));
-            r.v[0] = __uint_as_float(t.x << 16);
-            r.v[1] = __uint_as_float(t.x & 0xFFFF0000u);
-            r.v[2] = __uint_as_float(t.y << 16);
-            r.v[3] = __uint_as_float(t.y & 0xFFFF0000u);
-        } else {
-            const uint32_t t = __ldcg(reinterpret_cast<const unsigned int *>(p));
-            r.v[0] = __uint_as_float(t << 16);
-            r.v[1] = __uint_as_float(t & 0xFFFF0000u);
-        }
-    }
-    // One multiply-xorshift of the salt per row write (the salts already differ
-    // by row, pair and lane); each 32-bit word of noise rounds two elements (low
-    // half for the even element, high half for the odd one), the next word comes
-    // from one LCG step.  The rounding is bf16_sr_bits, done by the stochastic-
-    // rounding convert (cvt.rs.bf16x2.f32: upper result = a rounded with
-    // rbits[31:16], lower = b with rbits[15:0]), which gives bf16_sr_bits'
-    // result for every non-NaN input (infinities kept; a NaN stays a NaN).
-    __device__ __forceinline__ void store_bits(int32_t w, uint32_t lane, const RowVec<VEC> &r, uint32_t salt) const {
-        uint32_t word[VEC / 2];
-        uint32_t x = salt * 0x9E3779B1u;
-        x ^= x >> 16;
-#pragma unroll
-        for (int i = 0; i < VEC; i += 2) {
-            asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(word[i / 2]) : "f"(r.v[i + 1]), "f"(r.v[i]), "r"(x));
-            x = x * 0x9E3779B1u + 0x7F4A7C15u;
-        }
-        uint16_t *p = reinterpret_cast<uint16_t *>(bf + (size_t)w * d + lane * VEC);
-        if constexpr (VEC == 8) {
-            __stcg(reinterpret_cast<uint4 *>(p), make_uint4(word[0], word[1], word[2], word[3]));
-        } else if constexpr (VEC == 4) {
-            __stcg(reinterpret_cast<uint2 *>(p), make_uint2(word[0], word[1]));
-        } else {
-            __stcg(reinterpret_cast<unsigned int *>(p), word[0]);
-        }
-    }
-    // Hogwild write of an updated row: FP32 masters (the hottest rows, where
-    // writers collide) receive `delta` by vector atomics; a BF16 row is stored
-    // as the warp's updated copy `value` (loaded at the start of the pair, so an
-    // update another warp made to the same cold row in that window is lost, as
-    // in any Hogwild scheme), rounded stochastically -- a store, not a
-    // read-modify-write, so the warp does not wait on it.
-    __device__ __forceinline__ void update(int32_t w, uint32_t lane, const RowVec<VEC> &delta,
-                                           const RowVec<VEC> &value, uint32_t salt) const {
-        if ((uint32_t)w < n_master) add_row<VEC>(master + (size_t)w * d + lane * VEC, delta);
-        else store_bits(w, lane, value, salt);
-    }
-    // row = value (one writer: deterministic mode).
-    __device__ __forceinline__ void put(int32_t w, uint32_t lane, const RowVec<VEC> &v, uint32_t salt) const {
-        if ((uint32_t)w < n_master) store_row<VEC>(master + (size_t)w * d + lane * VEC, v);
-        else store_bits(w, lane, v, salt);
-    }
-};
-
 // ------------------------------------------ plain rule, rows staged ahead
 
 // Hogwild form of the plain rule whose row loads overlap the previous pairs'
@@ -1518,10 +1422,12 @@ extern "C" int dg_sgns_create(const dg_sgns_params *p, uint32_t v_num, const uin
     DG_CHECK(p->window >= 1 && p->window <= 64, DG_ERR_ARG, "window %d out of range [1, 64]", p->window);
     DG_CHECK(p->negative >= 0 && p->negative <= 64, DG_ERR_ARG, "negative %d out of range [0, 64]", p->negative);
     DG_CHECK(p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH || p->mode == DG_SGNS_PLAIN_BF16 ||
-                 p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED,
+                 p->mode == DG_SGNS_CBOW || p->mode == DG_SGNS_SG_SHARED || p->mode == DG_SGNS_CBOW_BF16,
              DG_ERR_ARG, "unknown mode %d", p->mode);
-    DG_CHECK(p->mode != DG_SGNS_CBOW || p->negative <= kCbowMaxNeg, DG_ERR_ARG, "the CBOW trainer supports negative <= %d",
-             kCbowMaxNeg);
+    DG_CHECK((p->mode != DG_SGNS_CBOW && p->mode != DG_SGNS_CBOW_BF16) || p->negative <= kCbowMaxNeg, DG_ERR_ARG,
+             "the CBOW trainer supports negative <= %d", kCbowMaxNeg);
+    DG_CHECK(p->mode != DG_SGNS_CBOW_BF16 || p->size == 64 || p->size == 128 || p->size == 256, DG_ERR_ARG,
+             "the BF16 CBOW trainer supports size 64, 128 or 256");
     DG_CHECK(p->mode != DG_SGNS_SG_SHARED || p->negative <= kShareMaxNeg, DG_ERR_ARG,
              "the shared-negative trainer supports negative <= %d", kShareMaxNeg);
     DG_CHECK(p->deterministic != 2 || p->mode == DG_SGNS_PLAIN || p->mode == DG_SGNS_MINIBATCH ||
@@ -1671,7 +1577,7 @@ static int train_walks(dg_sgns *s, const dgs::WalkSet &ws, float alpha, dg_train
             adj_pairs += np;
         } else {
             rc = s->p.mode == DG_SGNS_MINIBATCH   ? launch_minibatch(s, a, ws)
-                 : s->p.mode == DG_SGNS_CBOW      ? launch_cbow(s, a, ws)
+                 : s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_CBOW_BF16 ? launch_cbow(s, a, ws)
                  : s->p.mode == DG_SGNS_SG_SHARED ? launch_negshare(s, a, ws)
                                                   : launch_plain(s, a, ws);
         }
@@ -1703,8 +1609,8 @@ extern "C" int dg_sgns_train_paths(dg_sgns *s, const dg_paths *paths, float alph
 extern "C" int dg_sgns_autotune(dg_sgns *s, const dg_paths *paths, dg_tune_info *info) {
     DG_CHECK(s && paths, DG_ERR_ARG, "dg_sgns_autotune: NULL argument");
     dg_tune_info r{};
-    if (s->p.mode == DG_SGNS_MINIBATCH || s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_SG_SHARED ||
-        s->p.deterministic || s->p.negative > dgs::kFastNeg || s->p.hs) {
+    if (s->p.mode == DG_SGNS_MINIBATCH || s->p.mode == DG_SGNS_CBOW || s->p.mode == DG_SGNS_CBOW_BF16 ||
+        s->p.mode == DG_SGNS_SG_SHARED || s->p.deterministic || s->p.negative > dgs::kFastNeg || s->p.hs) {
         r.n_candidates = 1;
         r.chosen = 0;
         if (info) *info = r;

@@ -2,7 +2,7 @@
 // device-resident walks, one warp per walk (lane l owns columns
 // [l*VEC, l*VEC+VEC) of every row):
 //
-//  * DG_SGNS_CBOW: cbow_kernel (word2vec.cu:401-509), the reference's default
+//  * DG_SGNS_CBOW (DG_SGNS_CBOW_BF16 on BF16 rows): cbow_kernel (word2vec.cu:401-509), the reference's default
 //    trainer (cbow = 1, word2vec.cu:59).  Per centre: the mean of the shrunk
 //    window's context rows, one positive and `negative` sampled targets, their
 //    gradient e added to every context row.
@@ -83,16 +83,35 @@ __device__ __forceinline__ void hs_path(const SgnsArgs &a, int32_t word, const R
 // per pass at four 256-thread blocks and three target rows in flight, 64.8 ms
 // at two blocks and six rows).
 constexpr int cbow_min_blocks(int vec) { return vec <= 4 ? 4 : 1; }
+// Target rows in flight per group: BF16 rows (BF) hold more registers per row
+// (the decoded copy and its noise), so size 128 takes two at a time there.
+constexpr int cbow_group(int vec, bool bf) { return vec == 4 ? (bf ? 2 : 3) : vec <= 2 ? 4 : 2; }
 
 // G: target rows fetched together (their loads overlap); later groups are
 // fetched after the earlier ones are written.
-template <int VEC, int G>
+// BF = true: DG_SGNS_CBOW_BF16, the same rule on BF16 rows (FP32 arithmetic;
+// FP32 master rows for the hottest words, updated by vector atomics; a BF16 row
+// is written as its re-read value plus the update, rounded stochastically with
+// noise keyed by row, walk, centre and target or window slot).
+template <int VEC, int G, bool BF>
 __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
     const uint32_t lane = threadIdx.x & 31;
     int32_t *sen = sen_all[threadIdx.x >> 5];
     const int d = 32 * VEC;
     const uint32_t w = (uint32_t)a.window;
+    const BfRows<VEC> in{a.in_bf, a.in_master, a.n_master, d};
+    const BfRows<VEC> out{a.out_bf, a.out_master, a.n_master, d};
+    const uint32_t key = a.seed_lo ^ bf_mix(a.pass * 0x9E3779B9u + 0x5851F42Du);
+    // Row `id` of the input (context) or output table, this lane's columns.
+    auto load_in = [&](int32_t id, RowVec<VEC> &r) {
+        if constexpr (BF) in.load(id, lane, r);
+        else load_row<VEC>(a.syn0 + (size_t)id * d + lane * VEC, r);
+    };
+    auto load_out = [&](int32_t id, RowVec<VEC> &r) {
+        if constexpr (BF) out.load(id, lane, r);
+        else load_row<VEC>(a.syn1 + (size_t)id * d + lane * VEC, r);
+    };
     unsigned long long n_words = 0, n_trained = 0, n_pairs = 0;
     for (;;) {
         uint32_t walk = 0;
@@ -119,8 +138,7 @@ __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_k
                 RowVec<VEC> r[4];
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (s + k < hi && s + k != w)
-                        load_row<VEC>(a.syn0 + (size_t)sen[p - w + s + k] * d + lane * VEC, r[k]);
+                    if (s + k < hi && s + k != w) load_in(sen[p - w + s + k], r[k]);
 #pragma unroll
                 for (int k = 0; k < 4; k++)
                     if (s + k < hi && s + k != w) {
@@ -138,7 +156,8 @@ __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_k
             const int nt = 1 + (a.vocab_size > 1 ? a.negative : 0);
             RowVec<VEC> e;
             zero_row(e);
-            if (a.hs) hs_path<VEC>(a, word, neu1, e, lane);
+            if (!BF && a.hs) hs_path<VEC>(a, word, neu1, e, lane);
+            const uint32_t base = BF ? bf_mix(key ^ bf_mix(wid * 0x01000193u + p * 0x2545F491u) ^ lane * 0x85EBCA6Bu) : 0u;
             for (int g0 = 0; g0 < nt; g0 += G) {
                 int32_t t[G];
                 RowVec<VEC> row[G];
@@ -147,7 +166,7 @@ __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_k
                     const int j = g0 + k;
                     t[k] = j >= nt ? -1 : j == 0 ? word : __shfl_sync(0xffffffffu, mine, (j - 1) & 31);
                     if (j > 0 && t[k] == word) t[k] = -1;
-                    if (t[k] >= 0) load_row<VEC>(a.syn1 + (size_t)t[k] * d + lane * VEC, row[k]);
+                    if (t[k] >= 0) load_out(t[k], row[k]);
                 }
 #pragma unroll
                 for (int k = 0; k < G; k++) {
@@ -160,9 +179,15 @@ __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_k
                         upd.v[i] = __fmul_rn(g, neu1.v[i]);
                         row[k].v[i] += upd.v[i];
                     }
-                    float *rp = a.syn1 + (size_t)t[k] * d + lane * VEC;
-                    if (a.deterministic) store_row<VEC>(rp, row[k]);
-                    else add_row<VEC>(rp, upd);
+                    if constexpr (BF) {
+                        const uint32_t salt = base + (uint32_t)t[k] * 0x27D4EB2Fu + (uint32_t)(g0 + k);
+                        if (a.deterministic) out.put(t[k], lane, row[k], salt);
+                        else out.update(t[k], lane, upd, row[k], salt);
+                    } else {
+                        float *rp = a.syn1 + (size_t)t[k] * d + lane * VEC;
+                        if (a.deterministic) store_row<VEC>(rp, row[k]);
+                        else add_row<VEC>(rp, upd);
+                    }
                     // A repeat of this target later in the group sees this update.
 #pragma unroll
                     for (int q = k + 1; q < G; q++)
@@ -172,6 +197,20 @@ __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_k
             // e to every context row, in window order (word2vec.cu:498-505).
             for (uint32_t s = lo; s < hi; s++) {
                 if (s == w) continue;
+                if constexpr (BF) {
+                    // The row as it is now (a repeat of a context word in the
+                    // window sees the earlier slot's store), plus e.
+                    const int32_t cw = sen[p - w + s];
+                    RowVec<VEC> r;
+                    zero_row(r);
+                    if ((uint32_t)cw >= a.n_master || a.deterministic) in.load(cw, lane, r);
+#pragma unroll
+                    for (int i = 0; i < VEC; i++) r.v[i] = r.v[i] + e.v[i];
+                    const uint32_t salt = base + (uint32_t)cw * 0x165667B1u + s * 16u + 15u;
+                    if (a.deterministic) in.put(cw, lane, r, salt);
+                    else in.update(cw, lane, e, r, salt);
+                    continue;
+                }
                 float *cp = a.syn0 + (size_t)sen[p - w + s] * d + lane * VEC;
                 if (a.deterministic) {
                     RowVec<VEC> r;
@@ -404,10 +443,10 @@ static int worker_blocks(const dg_sgns *s, int resident, int threads) {
     return std::max(1, std::min(resident, want));
 }
 
-template <int V>
+template <int V, bool BF>
 static int cbow_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
-    constexpr int G = V == 4 ? 3 : V <= 2 ? 4 : 2;
-    auto kern = sgns_cbow_kernel<V, G>;
+    constexpr int G = cbow_group(V, BF);
+    auto kern = sgns_cbow_kernel<V, G, BF>;
     const int threads = w2v_threads(s);
     const int blocks = s->p.deterministic ? 1 : worker_blocks(s, resident_blocks(kern, threads, 0, s->device), threads);
     kern<<<blocks, threads, 0, s->stream>>>(a, ws);
@@ -428,12 +467,20 @@ static int negshare_launch(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
 }
 
 int launch_cbow(dg_sgns *s, const SgnsArgs &a, const WalkSet &ws) {
+    if (s->p.mode == DG_SGNS_CBOW_BF16) {
+        switch (s->p.size / 32) {
+            case 2: return cbow_launch<2, true>(s, a, ws);
+            case 4: return cbow_launch<4, true>(s, a, ws);
+            case 8: return cbow_launch<8, true>(s, a, ws);
+            default: return dg::fail(DG_ERR_ARG, "size %d not supported on BF16 rows (64, 128, 256)", s->p.size);
+        }
+    }
     switch (s->p.size / 32) {
-        case 1: return cbow_launch<1>(s, a, ws);
-        case 2: return cbow_launch<2>(s, a, ws);
-        case 4: return cbow_launch<4>(s, a, ws);
-        case 8: return cbow_launch<8>(s, a, ws);
-        case 16: return cbow_launch<16>(s, a, ws);
+        case 1: return cbow_launch<1, false>(s, a, ws);
+        case 2: return cbow_launch<2, false>(s, a, ws);
+        case 4: return cbow_launch<4, false>(s, a, ws);
+        case 8: return cbow_launch<8, false>(s, a, ws);
+        case 16: return cbow_launch<16, false>(s, a, ws);
         default: return dg::fail(DG_ERR_ARG, "size %d not supported (32, 64, 128, 256, 512)", s->p.size);
     }
 }

@@ -19,7 +19,7 @@ import numpy as np
 from . import _lib
 from ._lib import check, lib
 
-MODES = {"plain": 0, "minibatch": 1, "plain_bf16": 2, "cbow": 3, "sg_shared": 4}
+MODES = {"plain": 0, "minibatch": 1, "plain_bf16": 2, "cbow": 3, "sg_shared": 4, "cbow_bf16": 5}
 
 
 class SGNS:

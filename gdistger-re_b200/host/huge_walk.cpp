@@ -26,9 +26,10 @@
 //   -hs 0|1 (default 0, word2vec.cu:66): hierarchical softmax before negative sampling
 //   -binary: only 0 is supported (text output)
 // Added for the GPU build:
-//   -mode plain|plain_bf16|minibatch|cbow|sg_shared   trainer form, overriding -cbow /
-//                           -reuse-neg (plain = skip_gram_kernel on FP32 rows;
-//                           plain_bf16: the same rule on BF16 rows; minibatch: dsgl)
+//   -mode plain|plain_bf16|minibatch|cbow|cbow_bf16|sg_shared   trainer form,
+//                           overriding -cbow / -reuse-neg (plain = skip_gram_kernel on
+//                           FP32 rows; plain_bf16 / cbow_bf16: the rule on BF16 rows;
+//                           minibatch: dsgl)
 //   -lr exp|fixed|cosine|step|custom   per-round schedule (default exp, decay 0.1)
 //   -lr-start a             the schedule's first rate (default 0.025, word2vec.cu:1279;
 //                           -alpha does not change it, as in the reference)
@@ -138,14 +139,14 @@ Options parse(int argc, char **argv) {
     if (o.graph.empty() || o.v_num == 0 || o.walker_num == 0)
         die("usage: huge_walk -g edges.bin -v V -w W [--min_L L] [--min_R R] [--make-undirected] [-o prefix] "
             "[-size d -window k -negative n -batch-size b -sample s -alpha a -iter i -min-count c "
-            "-emb_output file] [-cbow 0|1 -reuse-neg 0|1] [-mode plain|plain_bf16|minibatch|cbow|sg_shared]");
+            "-emb_output file] [-cbow 0|1 -reuse-neg 0|1] [-mode plain|plain_bf16|minibatch|cbow|cbow_bf16|sg_shared]");
     if (o.mode.empty()) o.mode = o.cbow ? "cbow" : o.reuse_neg ? "sg_shared" : "plain";
     // word2vec.cu:1554-1555: -cbow 1 sets alpha = 0.05 unless -alpha is given (the
     // per-round schedule then overrides it, word2vec.cu:1290).
-    if (o.mode == "cbow" && !o.alpha_set) o.alpha = 0.05f;
+    if ((o.mode == "cbow" || o.mode == "cbow_bf16") && !o.alpha_set) o.alpha = 0.05f;
     if (o.mode != "plain" && o.mode != "minibatch" && o.mode != "plain_bf16" && o.mode != "cbow" &&
-        o.mode != "sg_shared")
-        die("-mode must be plain, plain_bf16, minibatch, cbow or sg_shared");
+        o.mode != "cbow_bf16" && o.mode != "sg_shared")
+        die("-mode must be plain, plain_bf16, minibatch, cbow, cbow_bf16 or sg_shared");
     if (o.rounds < 1 || o.rounds > 30) die("-rounds must be 1..30 (walk.hpp:740 stops after round 30)");
     return o;
 }
@@ -196,6 +197,7 @@ int main(int argc, char **argv) {
     sp.mode = o.mode == "plain"        ? DG_SGNS_PLAIN
               : o.mode == "plain_bf16" ? DG_SGNS_PLAIN_BF16
               : o.mode == "cbow"       ? DG_SGNS_CBOW
+              : o.mode == "cbow_bf16"  ? DG_SGNS_CBOW_BF16
               : o.mode == "sg_shared"  ? DG_SGNS_SG_SHARED
                                        : DG_SGNS_MINIBATCH;
     sp.deterministic = o.deterministic;

@@ -143,6 +143,9 @@ enum {
     DG_SGNS_SG_SHARED = 4,  /* word2vec.cu __sgNegReuse semantics (-cbow 0 -reuse-neg 1): FP32 rows, one negative
                                set per walk, the full window; negative <= 16.  Every supported size (the
                                reference builds only 200 and 300) */
+    DG_SGNS_CBOW_BF16 = 5,  /* DG_SGNS_CBOW's rule on BF16 rows: FP32 arithmetic, FP32 master rows for the
+                               master_rows most frequent words, stochastic rounding of every BF16 row write;
+                               size 64, 128 or 256, negative <= 32, no hierarchical softmax */
 };
 
 typedef struct {

@@ -162,3 +162,57 @@ def test_hierarchical_softmax_bit_exact(oracle, rule, negative):
     assert np.array_equal(rows.view(np.uint32), o.syn0_f32.view(np.uint32))
     assert np.array_equal(s.output_rows().view(np.uint32), o.syn1_f32.view(np.uint32))
     assert pairs == o.stats_f32.pairs
+
+
+@pytest.mark.parametrize("size", [64, 128, 256])
+def test_cbow_bf16_deterministic_error_stated(oracle, size):
+    """CBOW on BF16 rows (DG_SGNS_CBOW_BF16), one warp: the same walks, centres
+    and counters as the FP32 restatement; the rows differ only by the BF16
+    storage (stochastic rounding of every row write, FP32 masters for the 16
+    most frequent words): relative Frobenius error against the restatement's FP32
+    rows <= 5 % after two passes, while training moved the rows more than 10x
+    that from their initial values."""
+    offs, verts, counts = _walks(oracle)
+    cfg = dict(size=size, window=5, negative=5)
+    kw = dict(sample=1e-3, alpha=0.05, min_count=0, seed=7, table_size=100_000)
+    s = SGNS(200, counts, mode="cbow_bf16", deterministic=True, master_rows=16, **cfg, **kw)
+    assert s.master_rows == 16
+    o = oracle.Sgns(counts, **cfg, **kw)
+    init = o.syn0_f32.copy()
+    words = pairs = 0
+    for it in range(2):
+        info = s.train_host(offs, verts)
+        words += info.words
+        pairs += info.pairs
+        o.train(offs, verts, rule="cbow")
+    assert (words, pairs) == (o.stats_f32.words, o.stats_f32.pairs)
+    rows, _ = s.embedding()
+    out = s.output_rows()
+    err = max(_rel(rows, o.syn0_f32), _rel(out, o.syn1_f32))
+    moved = _rel(o.syn0_f32, init)
+    print(f"CBOW BF16 d={size}: error {err:.3e}, rows moved {moved:.3e}")
+    assert err < 5e-2
+    assert moved > 10 * _rel(rows, o.syn0_f32)
+
+
+def test_cbow_bf16_hogwild_round(distger_lib, round10k):
+    """Hogwild CBOW on BF16 rows over a round of the 10,000-vertex graph: the FP32
+    CBOW run's counters, finite rows of the same scale (norms within 5 % of the
+    FP32 rows')."""
+    p, counts = round10k
+
+    def run(mode):
+        s = SGNS(10_000, counts, size=128, window=10, negative=5, sample=1e-3, alpha=0.025, min_count=0, seed=3,
+                 table_size=1_000_000, mode=mode)
+        info = s.train_paths(p)
+        out = (info, s.embedding()[0], s.output_rows())
+        s.close()
+        return out
+
+    f32, bf = run("cbow"), run("cbow_bf16")
+    assert (f32[0].words, f32[0].trained, f32[0].pairs) == (bf[0].words, bf[0].trained, bf[0].pairs)
+    assert np.isfinite(bf[1]).all() and np.isfinite(bf[2]).all()
+    for a, b in ((bf[1], f32[1]), (bf[2], f32[2])):
+        r = np.linalg.norm(a) / np.linalg.norm(b)
+        print(f"CBOW BF16 / FP32 norm ratio {r:.4f}")
+        assert abs(r - 1) < 0.05, r

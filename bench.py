@@ -267,10 +267,13 @@ C5_REF_HOST_GB = 1.47e9 * (12 + 24 + 16 + 16) / 1e9 + 60
 
 def c5_reference_blocker(tmpdir=None) -> str | None:
     """Why the reference's walk engine does not run the Twitter-shaped graph here."""
-    return (f"the reference walk engine must load all 1.47e9 edges first: about {C5_REF_HOST_GB:.0f} GB of host "
-            f"memory at its peak (records, undirected doubling, CSR and co-occurrence CSR, graph.hpp:376-472, "
-            f"642-824; this host has {host_memory_gb():.0f} GB available) and single-threaded passes over "
-            f"2.94e9 CSR entries, far beyond the minutes a bench run may take")
+    return (f"too slow for a bench run: one walk round of the reference engine over the 41.6M walkers is "
+            f"~916M footprints, at the ~3.4M steps/s it reaches on the YouTube-shaped graph on this box's cores about "
+            f"4.5 minutes a round ("
+            f"{3 + 5} rounds for the default warm-up and steps), after single-threaded load passes over the "
+            f"1.47e9 edges and their 2.94e9 CSR entries, with about {C5_REF_HOST_GB:.0f} GB of host memory at "
+            f"its peak (records, undirected doubling, CSR and co-occurrence CSR, graph.hpp:376-472, 642-824; "
+            f"{host_memory_gb():.0f} GB available here)")
 
 
 def cpu_baseline(args, wl, graph, host_edges):

@@ -1,13 +1,18 @@
 #!/usr/bin/env python
 """Benchmark of DistGER's embedding hot path on B200: walk rounds streamed into SGNS.
 
-Workload (N=1): the YouTube-shaped graph -- Chung-Lu power law, exponent 2.1,
-1,138,499 vertices, ~2.99M undirected edges (3.25M records after the generator's
-isolated-vertex fix), max expected degree 28,000, edge data uniform(0,1] FP32 --
-with the reference walk defaults (--min_L 20, w = V walkers per round) and SGNS
-d=128, window 10, negative 5, sample 1e-3, alpha 0.01, iter 1, FP32 Hogwild (the
-plain form).  One step = one walk round of V walks + SGNS over those walks.
-Synthetic data: none of the paper's graphs ship with the reference.
+Workload (N=1, the default): the Twitter-shaped graph -- Chung-Lu power law,
+exponent 1.9, 41,652,230 vertices, 2.417e9 edge draws leaving ~1.47e9 unique
+undirected edges, expected degrees capped at 3M, unweighted, generated and built
+into the CSR on the device -- with the reference walk defaults (--min_L 20,
+--min_R 5, w = V walkers per round, walks of at most 32 footprints) and SGNS
+d=128, window 10, negative 5, sample 1e-3, alpha 0.01, iter 1; headline form:
+the plain rule on BF16 rows with FP32 masters, FP32 plain measured beside it.
+--bench-workload c2_youtube (1,138,499 vertices, exponent 2.1, ~2.99M edges,
+FP32 plain) and c3_livejournal (2,238,731 vertices, exponent 2.3, 14M edge
+draws, BF16 against FP32) are the smaller lines.  One step = one walk round of
+V walks + SGNS over those walks.  Synthetic data: none of the paper's graphs
+ship with the reference.
 
 value  = walk-steps embedded per second: footprints walked and trained per
          second of device time (CUDA events from the walk launch to the end of

@@ -45,7 +45,8 @@ def split(edges: np.ndarray, v_num: int, frac: float = 0.1, seed: int = 2, max_t
     """Returns (train_edges in gtrain's output order, test_pairs int64[n, 2],
     test_labels int8[n]): positives first, in the order drawn, then negatives.
     Raises RuntimeError where gtrain would loop forever (no edge left whose
-    endpoints both keep a second edge, or no free vertex pair)."""
+    endpoints both keep a second edge, or no free vertex pair).  It reseeds the
+    process's C-library rand() (srand(seed)), as the tool does."""
     c = _libc()
     c.srand.argtypes = [ctypes.c_uint]
     c.rand.restype = ctypes.c_int

@@ -1743,8 +1743,11 @@ extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t 
                                   float alpha, dg_train_info *info) {
     DG_CHECK(s && offsets && (vertices || offsets[n_walks] == 0), DG_ERR_ARG, "dg_sgns_train_host: NULL argument");
     const uint64_t total = offsets[n_walks];
-    for (uint32_t i = 0; i < n_walks; i++)
+    uint64_t longest = 0;   // one pass over the offsets: order check and the longest walk
+    for (uint32_t i = 0; i < n_walks; i++) {
         DG_CHECK(offsets[i + 1] >= offsets[i], DG_ERR_ARG, "walk offsets decrease at walk %u", i);
+        longest = std::max<uint64_t>(longest, offsets[i + 1] - offsets[i]);
+    }
     dg::DeviceGuard guard(s->device);
     dg::DevArray<uint64_t> &d_off = s->host_off;
     dg::DevArray<uint32_t> &d_verts = s->host_verts;
@@ -1767,8 +1770,7 @@ extern "C" int dg_sgns_train_host(dg_sgns *s, const uint64_t *offsets, uint32_t 
     ws.verts = d_verts.p;
     ws.offsets = d_off.p;
     ws.n_walks = n_walks;
-    for (uint32_t i = 0; i < n_walks; i++)
-        ws.max_len = (uint32_t)std::max<uint64_t>(ws.max_len, std::min<uint64_t>(offsets[i + 1] - offsets[i], UINT32_MAX));
+    ws.max_len = (uint32_t)std::min<uint64_t>(longest, UINT32_MAX);
     ws.id_base = 0;
     return train_walks(s, ws, alpha, info);
 }

@@ -515,6 +515,9 @@ struct alignas(16) PipeWarp {
     float hist[S][32 * VEC];                      // updated context rows of the last S pairs
     int32_t sen[kPipeSentence];
     int32_t tb[S][(2 * kPipeMaxWindow + 1) * NS];  // negatives of S centres, ring by centre
+    // Per slot of those centres: bit j set when negative j trains (it exists and
+    // is not the centre's word); bit 15 when a negative repeats within the slot.
+    uint16_t fl[S][2 * kPipeMaxWindow + 1];
     uint16_t lohi[kPipeSentence];                 // slot range of each centre: lo | hi << 8
 };
 
@@ -622,6 +625,24 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
         auto enter = [&](uint32_t q) {   // the copies reach centre q: draw its negatives
             const uint32_t lo = sm.lohi[q] & 0xFFu, hi = sm.lohi[q] >> 8;
             draw_negatives(a, q, wid, lo, hi, neg, sm.tb[q % S], NS);
+            {   // each slot's flags, once per centre instead of at every pair
+                const int32_t cw = sm.sen[q];
+                for (uint32_t k = lane; k < hi - lo; k += 32) {
+                    const int32_t *tk = sm.tb[q % S] + k * NS;
+                    uint32_t f = 0;
+#pragma unroll
+                    for (int j = 0; j < NS; j++) {
+                        if (j >= neg) break;
+                        const int32_t tj = tk[j];
+                        if (tj != cw) f |= 1u << j;
+#pragma unroll
+                        for (int i = 0; i < j; i++)
+                            if (tk[i] == tj) f |= 0x8000u;
+                    }
+                    sm.fl[q % S][k] = (uint16_t)f;   // slot w (no pair) gets an unused value
+                }
+                __syncwarp();
+            }
             if (lane == 0) {
                 const int32_t cw = sm.sen[q];
                 if (!BF) prefetch_l2(a.syn1 + (size_t)cw * D, (uint32_t)D * 4);
@@ -674,18 +695,16 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
 #pragma unroll
             for (int k = S - 1; k >= 0; k--)   // newest match last: it wins
                 if (hw[k] == last) lds_row<VEC>(&sm.hist[(mm + S - 1 - k) % S][lane * VEC], l1);
-            const int32_t *tq = sm.tb[p % S] + (s - (sm.lohi[p] & 0xFFu)) * NS;
+            const uint32_t ks = s - (sm.lohi[p] & 0xFFu);
+            const int32_t *tq = sm.tb[p % S] + ks * NS;
             int32_t t[NS];
 #pragma unroll
             for (int j = 0; j < NS; j++) t[j] = j < neg ? tq[j] : -1;
 #pragma unroll
             for (int i = 0; i < VEC; i++) e.v[i] = 0.f;
             n_pairs++;
-            bool repeat = false;
-#pragma unroll
-            for (int j = 0; j < NS; j++)
-#pragma unroll
-                for (int k = j + 1; k < NS; k++) repeat |= k < neg && t[k] == t[j];
+            const uint32_t flags = sm.fl[p % S][ks];
+            const bool repeat = (flags & 0x8000u) != 0;
             // Writes negative j's row: an atomic delta (FP32 rows, masters) or the
             // warp's updated copy (BF16 rows).
             auto write_neg = [&](int j, const RowVec<VEC> &upd, const RowVec<VEC> &value) {
@@ -700,7 +719,7 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
                     for (int i = 0; i < VEC; i++) s0 = fmaf(l1.v[i], pos.v[i], s0);
                     f[0] = s0;
                 }
-                uint32_t live = 0;
+                const uint32_t live = flags & 0xFFu;
                 // BF16 rows: decoded once and kept for the update phase (FP32 rows
                 // are read from shared memory again instead, to save registers).
                 RowVec<VEC> kept[BF ? NS : 1];
@@ -712,7 +731,6 @@ __global__ void __launch_bounds__(THREADS, FIT > 0 ? FIT : 1) sgns_plain_pipe_ke
                         read_slot(&sm.stage[st][1 + j][lane * VEC], t[j], false, r);
 #pragma unroll
                         for (int i = 0; i < VEC; i++) sj = fmaf(l1.v[i], r.v[i], sj);
-                        if (t[j] != word) live |= 1u << j;
                         if constexpr (BF) kept[j] = r;
                     }
                     f[j + 1] = sj;

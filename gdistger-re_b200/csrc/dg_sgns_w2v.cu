@@ -90,9 +90,11 @@ constexpr int cbow_group(int vec, bool bf) { return vec == 4 ? (bf ? 2 : 3) : ve
 // G: target rows fetched together (their loads overlap); later groups are
 // fetched after the earlier ones are written.
 // BF = true: DG_SGNS_CBOW_BF16, the same rule on BF16 rows (FP32 arithmetic;
-// FP32 master rows for the hottest words, updated by vector atomics; a BF16 row
-// is written as its re-read value plus the update, rounded stochastically with
-// noise keyed by row, walk, centre and target or window slot).
+// FP32 master rows for the hottest words, updated by vector atomics; a BF16
+// target row is written as the copy loaded for its dot product plus the update,
+// a BF16 context row as its value re-read before the write plus e, each rounded
+// stochastically with noise keyed by row, walk, centre and target or window
+// slot).
 template <int VEC, int G, bool BF>
 __global__ void __launch_bounds__(kW2vThreads, cbow_min_blocks(VEC)) sgns_cbow_kernel(SgnsArgs a, WalkSet ws) {
     __shared__ int32_t sen_all[kW2vThreads / 32][kMaxSentence];
